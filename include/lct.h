@@ -1,0 +1,265 @@
+/*
+ * lct.h -- C ABI of the B200-native helical cone-beam FDK hot path (liblct.so).
+ *
+ * Plain C types only: device pointers are `float*`/`double*` the caller owns, streams are
+ * cudaStream_t passed as an opaque pointer, every function returns an lct status code
+ * (LCT_OK == 0).  Kernels are asynchronous on the given stream unless stated otherwise.
+ *
+ * Each entry point names the reference interface it replaces (file:line within the reference
+ * project ltldlzltl/LISTCTRecons).  The reference stage methods take a `const ReconData*` and
+ * work on buffers owned by its CTDataGPU (Include/DataStructs.h:207-229); the drop-in glue
+ * (listctrecons_b200/dropin/Stages.cpp) unpacks those buffers and calls the functions below.
+ */
+#ifndef LCT_H
+#define LCT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------------------
+ * Status codes
+ * ------------------------------------------------------------------------------------- */
+#define LCT_OK 0
+#define LCT_ERR_ARG 1         /* invalid argument or geometry */
+#define LCT_ERR_CUDA 2        /* CUDA runtime error; lct_last_cuda_error() has the code */
+#define LCT_ERR_ALLOC 3       /* device or host allocation failed */
+#define LCT_ERR_RANGE 4       /* planner: reconstruction outside the data range
+                                 (reference exits: Src/DataStructs.cpp:210-218) */
+#define LCT_ERR_DEVICE 5      /* a kernel raised the device status word */
+#define LCT_ERR_UNSUPPORTED 6 /* option not available for this geometry / build */
+#define LCT_ERR_IO 7          /* file missing or short */
+
+typedef void* lct_stream; /* cudaStream_t; NULL = the legacy default stream */
+
+/* Mirrors CTGeom (Include/DataStructs.h:15-107), field for field, same types. */
+typedef struct lct_geom {
+  float orbit, orbit_start; /* radians per view, angle of view 0 */
+  int ns, nt;               /* detector columns, rows */
+  float ws, wt;             /* central column, central row ((nt-1)/2) */
+  int n_angle, n_angle_add; /* rebinned views per block, fan views per block */
+  float ds, dt;             /* column / row spacing at iso (mm) */
+  float pitch;              /* table feed per rotation (mm) -- the .prm "PitchValue" */
+  float source_z0;          /* -pitch/2 */
+  float dso;                /* source to iso (mm) */
+  int n_proj_turn;          /* views per rotation */
+  int z_dir;                /* +1 / -1, direction of couch positions */
+  int add_projections;      /* extra fan views each side of a block */
+} lct_geom;
+
+/* Mirrors ImgGeom (Include/DataStructs.h:109-162). */
+typedef struct lct_img {
+  int nx, ny, nz;
+  float wx, wy, wz; /* voxel index of the origin: (n-1)/2 + offset, wz = 0 */
+  float dx, dy, dz;
+} lct_img;
+
+/* Interpolation: TEX8 reproduces the reference's texture sampling (its FP32 coordinate
+   arithmetic, 8-bit-fraction linear weights); EXACT uses FP64 geometry tables and full
+   FP32 weights. */
+#define LCT_INTERP_TEX8 0
+#define LCT_INTERP_EXACT 1
+
+/* Addressing outside the detector: BORDER reads 0 (cudaAddressModeBorder, the mode the
+   reference sets), CLAMP repeats the edge.  LEGACY (whole-pipeline option only) = CLAMP on
+   the first block and BORDER afterwards, which is what the reference's legacy texture
+   references did (attributes are captured at bind time and it assigns Border after the first
+   bind: CUDA/Rebiner.cu:137-139, CUDA/Backprojector.cu:134-136). */
+#define LCT_ADDR_BORDER 0
+#define LCT_ADDR_CLAMP 1
+#define LCT_ADDR_LEGACY 2
+
+/* ---------------------------------------------------------------------------------------
+ * Errors and device status
+ * ------------------------------------------------------------------------------------- */
+const char* lct_status_string(int status);
+int lct_last_cuda_error(void); /* cudaError_t of the last LCT_ERR_CUDA, per thread */
+/* Reads and clears the device status word that kernels raise on out-of-range work items
+   (no trap, no assert).  Synchronous. */
+int lct_device_status(int* code_out);
+int lct_version(void);
+
+/* ---------------------------------------------------------------------------------------
+ * Stage 1 -- rebinning.  fan [n_angle_add][nt][ns] -> par [n_angle][nt][ns] (both device).
+ * ------------------------------------------------------------------------------------- */
+/* HelicalConeBeamFan2ParRebinerGPU::rebin + rebin_fan2par_kernel (CUDA/Rebiner.cu:82-154) */
+int lct_rebin_fan2par(const lct_geom* g, const float* d_fan, float* d_par, int interp, int addr,
+                      lct_stream stream);
+/* The integer fan-view index and weight rebin_fan2par uses for every (ia, is), [n_angle][ns]
+   (diagnostic; same device code as lct_rebin_fan2par). */
+int lct_rebin_fan2par_index(const lct_geom* g, int interp, int32_t* d_idx, float* d_w,
+                            lct_stream stream);
+/* NullRebinerGPU::rebin + rebin_null_kernel (CUDA/Rebiner.cu:13-80) */
+int lct_rebin_null(const lct_geom* g, const float* d_fan, float* d_par, int addr,
+                   lct_stream stream);
+/* PiOriRebiner::rebin + rebin_pi_ori_kernel (CUDA/Rebiner.cu:156-233) */
+int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par, int interp, int addr,
+                     lct_stream stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Stage 2 -- pre-weighting, in place on par [n_angle][nt][ns].
+ * ------------------------------------------------------------------------------------- */
+/* PiOriPreWeighting::weighting + weighting_pi_ori_kernel (CUDA/PreWeighting.cu:8-44).
+   (NULLPreWeighting, Include/PreWeighting.h:13-19, is a no-op and needs no entry point.) */
+int lct_weight_pi_ori(const lct_geom* g, float* d_par, lct_stream stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Stage 3 -- ramp filter.
+ * ------------------------------------------------------------------------------------- */
+#define LCT_FILTER_RAMLAK 0      /* RampFilterGPU::calculate_filter (Src/Filter.cpp:8-20) */
+#define LCT_FILTER_SHEPP_LOGAN 1 /* Shepp-Logan kernel, same scaling convention */
+
+/* Smooth window (Include/SmoothWindow.h is empty in the reference): a frequency window
+   applied to the taps' response.  NONE leaves the taps bit-identical to the reference's. */
+#define LCT_WINDOW_NONE 0
+#define LCT_WINDOW_HANN 1
+#define LCT_WINDOW_HAMMING 2
+#define LCT_WINDOW_COSINE 3
+
+/* Host: fills h[2*ns] (h[0] unused, h[ns] is the centre tap), FP64 evaluated, stored as
+   float.  Replaces Filter::calculate_filter (Include/Filter.h:9, Src/Filter.cpp:8-20). */
+int lct_filter_taps(int kind, int window, int ns, float ds, float* h);
+
+#define LCT_FILTER_FP32 0  /* FP32 FMA in the reference's summation order (bit-exact) */
+#define LCT_FILTER_BF16X3 1 /* Toeplitz GEMM on tcgen05, BF16 hi/lo split, FP32 accumulate */
+
+/* Filter::filter + filter_kernel (CUDA/Filter.cu:10-73): rows[r][is] <-
+   sum_k h[is-k+ns] * rows[r][k] for r < nrows, in place (device pointers; d_h has 2*ns). */
+int lct_filter_rows(int ns, const float* d_h, float* d_rows, int64_t nrows, int mode,
+                    lct_stream stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Stage 4 -- backprojection.  proj [n_angle][nt][ns] filtered (device), betas[n_angle]
+ * (device, radians, float as in the reference), img [nz][ny][nx] (device).
+ * ------------------------------------------------------------------------------------- */
+/* HelicalConeBeamFanRebinBackprojectorGPU::backproject + backprojection_cbct_par_kernel
+   (CUDA/Backprojector.cu:12-169; na1_half = n_proj_turn/2, dz per view = pitch/n_proj_turn). */
+int lct_backproject_par(const lct_geom* g, const lct_img* ig, const float* d_betas,
+                        const float* d_proj, float* d_img, int interp, int addr,
+                        lct_stream stream);
+/* PiOriBackprojectorGPU::backproject + backprojection_cbct_pi_ori_kernel
+   (CUDA/Backprojector.cu:171-307). */
+int lct_backproject_pi_ori(const lct_geom* g, const lct_img* ig, const float* d_betas,
+                           const float* d_proj, float* d_img, int interp, int addr,
+                           lct_stream stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Planner -- ReconData::convert_from_file_params (Src/DataStructs.cpp:121-250) and
+ * BlockInfo::update (Src/DataStructs.cpp:77-108), reproduced in the reference's FP32
+ * arithmetic with 64-bit sizes.
+ * ------------------------------------------------------------------------------------- */
+/* The .prm keys that reach the path (Src/FileParams.cpp:10), plus one optional key. */
+typedef struct lct_scan_params {
+  int ns, nt;
+  float ds, dt;
+  float pitch_value; /* PitchValue: / TableFeed: */
+  int nx, ny;
+  float dx, dz;
+  float offset_x, offset_y;
+  int readings, view_offset, data_offset;
+  float r_src_to_iso;
+  float central_channel;
+  int n_proj_turn;
+  int max_blocks; /* new optional key MaxBlocks: reconstruct only the first N blocks (0 = all) */
+} lct_scan_params;
+
+typedef struct lct_plan_info {
+  lct_geom ctg;
+  lct_img ig;
+  /* ReconInfo (Include/DataStructs.h:231-279) */
+  int n_readings;
+  float data_begin_pos, data_end_pos, allow_begin, allow_end, start_pos, end_pos;
+  float recon_start_pos, recon_end_pos;
+  int n_slices_recon, n_slices_block, n_blocks, data_offset;
+  int n_blocks_run; /* min(n_blocks, max_blocks) */
+} lct_plan_info;
+
+/* BlockInfo (Include/DataStructs.h:281-311) of one block. */
+typedef struct lct_block_info {
+  int block_idx;
+  int block_proj_start, block_proj_end;
+  float block_start, block_end;
+  int block_slice_start, block_slice_end;
+} lct_block_info;
+
+typedef struct lct_plan lct_plan;
+
+/* tube_angles / table_positions: `readings` floats each (the contents of ViewAngleFile and
+   CouchPosFile after ViewOffset), copied. */
+int lct_plan_create(const lct_scan_params* p, const float* tube_angles,
+                    const float* table_positions, lct_plan** out);
+int lct_plan_info_get(const lct_plan* plan, lct_plan_info* out);
+int lct_plan_block(const lct_plan* plan, int b, lct_block_info* out);
+void lct_plan_destroy(lct_plan* plan);
+
+/* ---------------------------------------------------------------------------------------
+ * Whole reconstruction -- FDKReconstructor::reconstruct (Src/Reconstructor.cpp:30-49) with
+ * the stages the factory builds (Src/ReconstructorAbstractFactory.cpp:11-33).
+ * ------------------------------------------------------------------------------------- */
+#define LCT_MODE_BLOCK 0 /* the reference's per-block flow (each block rebins/filters its own
+                            view window), on device-resident data */
+#define LCT_MODE_SCAN 1  /* each view is rebinned and filtered once; slabs backproject from
+                            the shared filtered views (FP64 rebin tables) */
+
+#define LCT_REBIN_FAN2PAR 0
+#define LCT_REBIN_NULL 1
+#define LCT_REBIN_PI_ORI 2
+#define LCT_PW_NONE 0
+#define LCT_PW_PI_ORI 1
+#define LCT_BP_PAR 0
+#define LCT_BP_PI_ORI 1
+
+typedef struct lct_recon_opts {
+  int mode;          /* LCT_MODE_* */
+  int rebinner;      /* LCT_REBIN_* */
+  int preweight;     /* LCT_PW_* */
+  int filter_kind;   /* LCT_FILTER_RAMLAK / SHEPP_LOGAN */
+  int window;        /* LCT_WINDOW_* */
+  int filter_mode;   /* LCT_FILTER_FP32 / BF16X3 */
+  int backprojector; /* LCT_BP_* */
+  int interp;        /* LCT_INTERP_* */
+  int addr;          /* LCT_ADDR_* */
+  int bp_nz;         /* backprojection slices per thread (0 = tuned) */
+} lct_recon_opts;
+
+void lct_recon_opts_default(lct_recon_opts* o);
+
+typedef struct lct_recon lct_recon;
+
+/* Allocates every device buffer the plan needs (no allocation happens in run). */
+int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out);
+/* Reconstructs n_blocks_run blocks.  fan: all `readings` views [readings][nt][ns] float
+   (host: pinned or pageable; device: a device pointer); image: [n_blocks_run*32][ny][nx]. */
+int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, float* image,
+                  int image_on_device, lct_stream stream);
+/* Device-side per-stage time of the last run (ms): h2d, rebin, filter, backproject, d2h. */
+int lct_recon_last_times(const lct_recon* r, float* ms5);
+/* Fan views [first, first+count) the run reads (h2d bytes = count*nt*ns*4). */
+int lct_recon_fan_range(const lct_recon* r, int64_t* first, int64_t* count);
+void lct_recon_destroy(lct_recon* r);
+
+/* ---------------------------------------------------------------------------------------
+ * Scan simulator (no reference counterpart): analytic helical fan-beam line integrals of
+ * an ellipsoid phantom with Poisson noise.  Ellipsoid record = 16 doubles:
+ * cx, cy, cz, ax, ay, az, rot[9] (row-major, ellipsoid frame -> world), mu (1/mm).
+ * ------------------------------------------------------------------------------------- */
+int lct_sim_project(const double* d_ellipsoids, int n_ellipsoids, int ns, int nt, float ds,
+                    float dt, float ws, float wt, float dso, const double* d_angles,
+                    const double* d_zpos, int64_t v0, int64_t v1, double i0, uint64_t seed,
+                    float* d_fan, lct_stream stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Diagnostics
+ * ------------------------------------------------------------------------------------- */
+/* Samples a 3-D float texture (cudaFilterModeLinear, unnormalised) through the texture
+   hardware: host vol [nz][ny][nx], host coords[3n] (x,y,z), host out[n].  Synchronous. */
+int lct_diag_tex3d_sample(const float* vol, int nx, int ny, int nz, const float* coords,
+                          int64_t n, int addr, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LCT_H */

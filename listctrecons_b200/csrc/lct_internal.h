@@ -1,0 +1,74 @@
+// Internal helpers shared by the liblct translation units (not installed, not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lct.h"
+
+#define LCT_API extern "C" __attribute__((visibility("default")))
+
+namespace lct {
+
+// Include/Common.h:3-4.  PI is a double literal there; where the reference evaluates an
+// expression in double because of it, the product does the same.
+constexpr double kRefPi = 3.141592653589793238462643383;
+constexpr int kBlockSlices = 32;
+
+// Thread-local record of the last CUDA error turned into LCT_ERR_CUDA.
+void set_cuda_error(cudaError_t e);
+int cuda_status(cudaError_t e);  // LCT_OK or LCT_ERR_CUDA (records e)
+int launch_status();             // cudaGetLastError() -> status
+
+// Device status word (file-scope __device__ int in common.cu).  Kernels raise it on a work
+// item they refuse (an index outside its buffer) instead of trapping.
+int* device_status_ptr();  // per current device, resolved with cudaGetSymbolAddress
+enum DeviceStatus : int {
+  kDevOk = 0,
+  kDevIndexRange = 1,  // an index computed from the geometry fell outside its buffer
+  kDevWaitTimeout = 2, // a bounded wait in a pipelined kernel ran out
+};
+
+// Validation of the mirrored reference structs.
+int check_geom(const lct_geom* g);
+int check_img(const lct_img* ig);
+
+// Per-slice view windows of the parallel-beam backprojection (CUDA/Backprojector.cu:37-42),
+// always evaluated in FP32 exactly as the reference does.
+struct BpWindow {
+  int a_min, a_mid, a_max;
+};
+BpWindow bp_window(const lct_geom& g, const lct_img& ig, int iz, float dz_per_view,
+                   int na1_half);
+
+// Launch description for the parallel-beam backprojection kernels (backproject.cu).
+constexpr int kBpMaxZ = 32;      // slices sharing one window table
+constexpr int kBpMaxSlabs = 256; // slabs in one launch (scan mode)
+struct BpLaunch {
+  const float* proj;   // filtered views; slab s's local view 0 is proj + slab_view[s]*view_stride
+  const float* betas;  // view angles; slab s's local view 0 is betas + slab_view[s]
+  float* img;          // slab s, local slice z -> img + (slab_z0[s] + z) * nx * ny
+  long long view_stride;
+  int n_angle;         // local views per slab
+  int nz;              // slices per slab (<= kBpMaxZ)
+  int n_slabs;
+  int slab_view[kBpMaxSlabs];
+  int slab_z0[kBpMaxSlabs];
+  int interp, addr;
+  int nz_thread;       // slices per thread (8, 16, 32; 0 = choose)
+};
+int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaStream_t s);
+
+// Rebinning, scan mode: each global parallel view g in [g0, g0 + nviews) is interpolated
+// from the fan buffer whose view 0 is global fan view `fan_first`, with the view shift of
+// column is taken from an FP64 table (alpha(is)/orbit), identical for every view.
+int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long fan_first,
+                              long long fan_count, float* d_par, long long g0,
+                              long long nviews, int interp, int addr, cudaStream_t s);
+
+// Filter over nrows rows of ns samples (filter.cu).
+int launch_filter_rows(int ns, const float* d_h, float* d_rows, long long nrows, int mode,
+                       cudaStream_t s);
+
+}  // namespace lct

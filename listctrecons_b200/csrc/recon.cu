@@ -1,0 +1,330 @@
+// Whole reconstruction: FDKReconstructor::reconstruct (Src/Reconstructor.cpp:30-49) with the
+// stages ReconstrctorAbstractFactory builds (Src/ReconstructorAbstractFactory.cpp:11-33).
+//
+// Ownership follows the reference's GPUMemoryCtrl model (Include/GPUMemoryCtrl.h:6-62): one
+// owner allocates each device buffer once, at lct_recon_create, sized from the plan; run()
+// never allocates.  Buffers:
+//   fan   fan views [fan_first, fan_first + fan_count) -- the union of every block's window
+//   par   rebinned views, filtered in place:
+//           block mode: n_angle views, reused by every block (the reference's projGpu)
+//           scan mode:  global parallel views [g_first, g_first + g_count), each once
+//   betas the ViewAngleFile contents (all readings); block b reads from
+//         block_proj_start + add_projections (CUDA/Backprojector.cu:145)
+//   img   n_blocks_run * 32 slices, block b at slice 32 b (CUDA/Backprojector.cu:158)
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "lct_internal.h"
+
+namespace lct {
+const float* plan_angles(const lct_plan* p);
+const lct_scan_params& plan_params(const lct_plan* p);
+}  // namespace lct
+
+struct lct_recon {
+  lct_plan_info info;
+  std::vector<lct_block_info> blocks;
+  lct_recon_opts o;
+  long long plane = 0;           // nt * ns
+  long long fan_first = 0, fan_count = 0;
+  long long g_first = 0, g_count = 0;  // scan mode
+  float* d_fan = nullptr;
+  float* d_par = nullptr;
+  float* d_betas = nullptr;
+  float* d_h = nullptr;
+  float* d_img = nullptr;
+  cudaEvent_t ev[6] = {};
+  float times[5] = {};
+  int device = 0;
+};
+
+namespace lct {
+
+static void free_recon(lct_recon* r) {
+  if (!r) return;
+  cudaFree(r->d_fan);
+  cudaFree(r->d_par);
+  cudaFree(r->d_betas);
+  cudaFree(r->d_h);
+  cudaFree(r->d_img);
+  for (auto& e : r->ev)
+    if (e) cudaEventDestroy(e);
+  delete r;
+}
+
+static int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
+  if (requested == 8 || requested == 16 || requested == 32) return requested;
+  // slices a view stays active for: (feed/2) / dz
+  const double act = 0.5 * (double)g.pitch / (double)ig.dz;
+  return act >= 20.0 ? 16 : 8;
+}
+
+static int block_addr(const lct_recon* r, int b) {
+  if (r->o.addr == LCT_ADDR_LEGACY) return b == 0 ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  return r->o.addr;
+}
+
+}  // namespace lct
+
+using namespace lct;
+
+LCT_API void lct_recon_opts_default(lct_recon_opts* o) {
+  if (!o) return;
+  o->mode = LCT_MODE_SCAN;
+  o->rebinner = LCT_REBIN_FAN2PAR;
+  o->preweight = LCT_PW_NONE;
+  o->filter_kind = LCT_FILTER_RAMLAK;
+  o->window = LCT_WINDOW_NONE;
+  o->filter_mode = LCT_FILTER_FP32;
+  o->backprojector = LCT_BP_PAR;
+  o->interp = LCT_INTERP_TEX8;
+  o->addr = LCT_ADDR_BORDER;
+  o->bp_nz = 0;
+}
+
+LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out) {
+  if (!plan || !out) return LCT_ERR_ARG;
+  *out = nullptr;
+  lct_recon_opts o;
+  if (opts)
+    o = *opts;
+  else
+    lct_recon_opts_default(&o);
+  if (o.mode != LCT_MODE_BLOCK && o.mode != LCT_MODE_SCAN) return LCT_ERR_ARG;
+  if (o.rebinner < LCT_REBIN_FAN2PAR || o.rebinner > LCT_REBIN_PI_ORI) return LCT_ERR_ARG;
+  if (o.preweight != LCT_PW_NONE && o.preweight != LCT_PW_PI_ORI) return LCT_ERR_ARG;
+  if (o.backprojector != LCT_BP_PAR && o.backprojector != LCT_BP_PI_ORI) return LCT_ERR_ARG;
+  if (o.interp != LCT_INTERP_TEX8 && o.interp != LCT_INTERP_EXACT) return LCT_ERR_ARG;
+  if (o.addr < LCT_ADDR_BORDER || o.addr > LCT_ADDR_LEGACY) return LCT_ERR_ARG;
+  if (o.filter_mode != LCT_FILTER_FP32 && o.filter_mode != LCT_FILTER_BF16X3) return LCT_ERR_ARG;
+  if (o.mode == LCT_MODE_SCAN && o.rebinner == LCT_REBIN_PI_ORI) return LCT_ERR_UNSUPPORTED;
+
+  lct_recon* r = new (std::nothrow) lct_recon;
+  if (!r) return LCT_ERR_ALLOC;
+  r->o = o;
+  lct_plan_info_get(plan, &r->info);
+  const lct_geom& g = r->info.ctg;
+  const int nb = r->info.n_blocks_run;
+  if (nb <= 0 || nb > kBpMaxSlabs) {
+    delete r;
+    return nb <= 0 ? LCT_ERR_RANGE : LCT_ERR_UNSUPPORTED;
+  }
+  for (int b = 0; b < nb; ++b) {
+    lct_block_info bi;
+    lct_plan_block(plan, b, &bi);
+    r->blocks.push_back(bi);
+  }
+  r->plane = (long long)g.nt * g.ns;
+  long long lo = r->blocks[0].block_proj_start, hi = lo + g.n_angle_add;
+  for (auto& bi : r->blocks) {
+    lo = std::min<long long>(lo, bi.block_proj_start);
+    hi = std::max<long long>(hi, (long long)bi.block_proj_start + g.n_angle_add);
+  }
+  const long long readings = r->info.n_readings;
+  const long long off = r->info.data_offset;
+  if (lo + off < 0 || hi + off > readings) {
+    // the reference would read outside the raw file here (Src/DataReader.cpp:14)
+    delete r;
+    return LCT_ERR_RANGE;
+  }
+  r->fan_first = lo;
+  r->fan_count = hi - lo;
+  r->g_first = lo + g.add_projections;
+  r->g_count = r->fan_count - 2LL * g.add_projections;
+  cudaGetDevice(&r->device);
+
+  int st = LCT_OK;
+  const long long par_views = o.mode == LCT_MODE_SCAN ? r->g_count : g.n_angle;
+  const size_t img_elems = (size_t)nb * kBlockSlices * r->info.ig.nx * r->info.ig.ny;
+  do {
+    if ((st = cuda_status(cudaMalloc(&r->d_fan, sizeof(float) * r->fan_count * r->plane)))) break;
+    if ((st = cuda_status(cudaMalloc(&r->d_par, sizeof(float) * par_views * r->plane)))) break;
+    if ((st = cuda_status(cudaMalloc(&r->d_betas, sizeof(float) * readings)))) break;
+    if ((st = cuda_status(cudaMalloc(&r->d_h, sizeof(float) * 2 * g.ns)))) break;
+    if ((st = cuda_status(cudaMalloc(&r->d_img, sizeof(float) * img_elems)))) break;
+    if ((st = cuda_status(cudaMemcpy(r->d_betas, plan_angles(plan), sizeof(float) * readings,
+                                     cudaMemcpyHostToDevice))))
+      break;
+    std::vector<float> h(2 * (size_t)g.ns);
+    if ((st = lct_filter_taps(o.filter_kind, o.window, g.ns, g.ds, h.data()))) break;
+    if ((st = cuda_status(cudaMemcpy(r->d_h, h.data(), sizeof(float) * h.size(),
+                                     cudaMemcpyHostToDevice))))
+      break;
+    for (auto& e : r->ev)
+      if ((st = cuda_status(cudaEventCreate(&e)))) break;
+  } while (0);
+  if (st) {
+    free_recon(r);
+    return st == LCT_ERR_CUDA && lct_last_cuda_error() == cudaErrorMemoryAllocation ? LCT_ERR_ALLOC : st;
+  }
+  *out = r;
+  return LCT_OK;
+}
+
+LCT_API int lct_recon_fan_range(const lct_recon* r, int64_t* first, int64_t* count) {
+  if (!r) return LCT_ERR_ARG;
+  if (first) *first = r->fan_first + r->info.data_offset;
+  if (count) *count = r->fan_count;
+  return LCT_OK;
+}
+
+LCT_API int lct_recon_last_times(const lct_recon* r, float* ms5) {
+  if (!r || !ms5) return LCT_ERR_ARG;
+  std::memcpy(ms5, r->times, sizeof(r->times));
+  return LCT_OK;
+}
+
+static int run_rebin(lct_recon* r, const lct_geom& g, const float* fan_block, float* par, int addr,
+                     cudaStream_t s) {
+  const int interp = r->o.interp;
+  switch (r->o.rebinner) {
+    case LCT_REBIN_NULL: return lct_rebin_null(&g, fan_block, par, addr, s);
+    case LCT_REBIN_PI_ORI: return lct_rebin_pi_ori(&g, fan_block, par, interp, addr, s);
+    default: return lct_rebin_fan2par(&g, fan_block, par, interp, addr, s);
+  }
+}
+
+LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, float* image,
+                          int image_on_device, lct_stream stream) {
+  if (!r || !fan || !image) return LCT_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  const int nb = r->info.n_blocks_run;
+  const long long off = r->info.data_offset;
+  int st;
+  if ((st = cuda_status(cudaEventRecord(r->ev[0], s)))) return st;
+
+  // fan views needed by the run (the union of the blocks' windows)
+  const float* d_fan;
+  if (fan_on_device) {
+    d_fan = fan + (r->fan_first + off) * r->plane;
+  } else {
+    if ((st = cuda_status(cudaMemcpyAsync(r->d_fan, fan + (r->fan_first + off) * r->plane,
+                                          sizeof(float) * r->fan_count * r->plane,
+                                          cudaMemcpyHostToDevice, s))))
+      return st;
+    d_fan = r->d_fan;
+  }
+  if ((st = cuda_status(cudaEventRecord(r->ev[1], s)))) return st;
+  float* d_img = image_on_device ? image : r->d_img;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  const int bp_nz = pick_bp_nz(g, ig, r->o.bp_nz);
+
+  if (r->o.mode == LCT_MODE_BLOCK) {
+    // stages interleave per block; the whole compute span is reported as backprojection
+    cudaEventRecord(r->ev[2], s);
+    cudaEventRecord(r->ev[3], s);
+    for (int b = 0; b < nb; ++b) {
+      const lct_block_info& bi = r->blocks[b];
+      const int addr = block_addr(r, b);
+      const float* fan_block = d_fan + (bi.block_proj_start - r->fan_first) * r->plane;
+      if ((st = run_rebin(r, g, fan_block, r->d_par, addr, s))) return st;
+      if (r->o.preweight == LCT_PW_PI_ORI && (st = lct_weight_pi_ori(&g, r->d_par, s))) return st;
+      if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, (long long)g.n_angle * g.nt,
+                                   r->o.filter_mode, s)))
+        return st;
+      const float* betas = r->d_betas + bi.block_proj_start + g.add_projections;
+      float* img_b = d_img + (long long)b * slab;
+      if (r->o.backprojector == LCT_BP_PI_ORI) {
+        st = lct_backproject_pi_ori(&g, &ig, betas, r->d_par, img_b, r->o.interp, addr, s);
+      } else {
+        BpLaunch L;
+        L.proj = r->d_par;
+        L.betas = betas;
+        L.img = img_b;
+        L.view_stride = r->plane;
+        L.n_angle = g.n_angle;
+        L.nz = kBlockSlices;
+        L.n_slabs = 1;
+        L.slab_view[0] = 0;
+        L.slab_z0[0] = 0;
+        L.interp = r->o.interp;
+        L.addr = addr;
+        L.nz_thread = bp_nz;
+        st = launch_bp_par(g, ig, L, s);
+      }
+      if (st) return st;
+    }
+    cudaEventRecord(r->ev[4], s);
+  } else {
+    // scan mode: rebin every global view once (FP64 per-column shifts), filter once
+    const long long fan_base = r->fan_first;  // d_fan view 0 == global fan view fan_first
+    const int addr0 = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+    if (r->o.rebinner == LCT_REBIN_NULL) {
+      lct_geom gg = g;
+      gg.n_angle = (int)r->g_count;
+      gg.n_angle_add = (int)r->fan_count;
+      if ((st = lct_rebin_null(&gg, d_fan, r->d_par, addr0, s))) return st;
+    } else {
+      if ((st = launch_rebin_fan2par_scan(g, d_fan, fan_base, r->fan_count, r->d_par, r->g_first,
+                                          r->g_count, r->o.interp, addr0, s)))
+        return st;
+    }
+    if (r->o.preweight == LCT_PW_PI_ORI) {
+      lct_geom gg = g;
+      gg.n_angle = (int)r->g_count;
+      gg.n_angle_add = (int)r->g_count;
+      if ((st = lct_weight_pi_ori(&gg, r->d_par, s))) return st;
+    }
+    if ((st = cuda_status(cudaEventRecord(r->ev[2], s)))) return st;
+    if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, r->g_count * g.nt, r->o.filter_mode, s)))
+      return st;
+    if ((st = cuda_status(cudaEventRecord(r->ev[3], s)))) return st;
+    if (r->o.backprojector == LCT_BP_PI_ORI) {
+      for (int b = 0; b < nb; ++b) {
+        const long long gv = r->blocks[b].block_proj_start + g.add_projections;
+        st = lct_backproject_pi_ori(&g, &ig, r->d_betas + gv, r->d_par + (gv - r->g_first) * r->plane,
+                                    d_img + (long long)b * slab, r->o.interp, block_addr(r, b), s);
+        if (st) return st;
+      }
+    } else {
+      // one launch over every slab; with LEGACY addressing slab 0 runs apart (clamped)
+      int b0 = 0;
+      while (b0 < nb) {
+        const int addr = block_addr(r, b0);
+        int b1 = b0 + 1;
+        while (b1 < nb && block_addr(r, b1) == addr) ++b1;
+        BpLaunch L;
+        L.proj = r->d_par;
+        L.betas = r->d_betas;
+        L.img = d_img;
+        L.view_stride = r->plane;
+        L.n_angle = g.n_angle;
+        L.nz = kBlockSlices;
+        L.n_slabs = b1 - b0;
+        for (int b = b0; b < b1; ++b) {
+          const long long gv = r->blocks[b].block_proj_start + g.add_projections;
+          L.slab_view[b - b0] = (int)(gv - r->g_first);
+          L.slab_z0[b - b0] = b * kBlockSlices;
+        }
+        L.interp = r->o.interp;
+        L.addr = addr;
+        L.nz_thread = bp_nz;
+        // betas are indexed by the same slab offset: shift the base by g_first
+        L.betas = r->d_betas + r->g_first;
+        if ((st = launch_bp_par(g, ig, L, s))) return st;
+        b0 = b1;
+      }
+    }
+    if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
+  }
+
+  if (!image_on_device) {
+    if ((st = cuda_status(cudaMemcpyAsync(image, r->d_img, sizeof(float) * nb * slab,
+                                          cudaMemcpyDeviceToHost, s))))
+      return st;
+  }
+  if ((st = cuda_status(cudaEventRecord(r->ev[5], s)))) return st;
+  if ((st = cuda_status(cudaEventSynchronize(r->ev[5])))) return st;
+  for (int i = 0; i < 5; ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r->ev[i], r->ev[i + 1]);
+    r->times[i] = ms;
+  }
+  return LCT_OK;
+}
+
+LCT_API void lct_recon_destroy(lct_recon* r) { free_recon(r); }

@@ -1,0 +1,61 @@
+"""The texture hardware's linear filter against its register-side emulation (TEX8 kernels and
+the oracle's TEXEMU mode): same texels, 8-bit fractional weights."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from listctrecons_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+
+def _hw(vol, coords, addr):
+    out = np.zeros(len(coords), dtype=np.float32)
+    vol = np.ascontiguousarray(vol, dtype=np.float32)
+    c = np.ascontiguousarray(coords, dtype=np.float32)
+    nz, ny, nx = vol.shape
+    capi.check(capi.load().lct_diag_tex3d_sample(vol.ctypes.data, nx, ny, nz, c.ctypes.data, len(c),
+                                                 addr, out.ctypes.data))
+    return out
+
+
+def test_weight_quantisation_rule(cuda):
+    # a ramp along x: the sample is i + weight exactly (in-range, y/z at texel centres)
+    nx = 4096
+    vol = np.tile(np.arange(nx, dtype=np.float32), (2, 2, 1))
+    rng = np.random.default_rng(1)
+    x = rng.uniform(0.5, nx - 1.5, 20000).astype(np.float32)
+    x = np.concatenate([x, (np.arange(1, 2049, dtype=np.float32) / 2048.0 + 100.5).astype(np.float32)])
+    coords = np.stack([x, np.full_like(x, 0.5), np.full_like(x, 0.5)], 1)
+    hw = _hw(vol, coords, capi.ADDR_BORDER).astype(np.float64)
+    fb = x.astype(np.float64) - 0.5
+    frac = fb - np.floor(fb)
+    near = np.floor(fb) + np.floor(frac * 256 + 0.5) / 256
+    trunc = np.floor(fb) + np.floor(frac * 256) / 256
+    e_near = np.abs(hw - near)
+    e_trunc = np.abs(hw - trunc)
+    print(f"max|hw-nearest|={e_near.max():.3e} max|hw-trunc|={e_trunc.max():.3e} "
+          f"mismatch nearest={np.mean(e_near > 1e-3):.4f} trunc={np.mean(e_trunc > 1e-3):.4f}")
+    np.save("/tmp/lct_tex_probe.npy", np.stack([x, hw]))
+    assert min(e_near.max(), e_trunc.max()) < 2e-3  # one of the two rules describes the hardware
+    # the emulation the product and the oracle use must be that rule
+    q = orc.lib().orc_get_tex_quant()
+    best = orc.Q_NEAREST if np.mean(e_near > 1e-3) <= np.mean(e_trunc > 1e-3) else orc.Q_TRUNC
+    assert q == best
+
+
+@pytest.mark.parametrize("addr", [capi.ADDR_BORDER, capi.ADDR_CLAMP])
+def test_trilinear_matches_emulation(cuda, addr):
+    rng = np.random.default_rng(5)
+    vol = rng.uniform(-1, 1, (6, 7, 9)).astype(np.float32)
+    n = 5000
+    coords = np.stack([rng.uniform(-1.0, 10.0, n), rng.uniform(-1.0, 8.0, n),
+                       rng.uniform(-1.0, 7.0, n)], 1).astype(np.float32)
+    hw = _hw(vol, coords, addr)
+    emu = orc.tex3d_sample(vol, coords, orc.TEXEMU, addr)
+    exact = orc.tex3d_sample(vol, coords, orc.EXACT, addr)
+    e_emu = np.abs(hw - emu).max()
+    e_exact = np.abs(hw - exact).max()
+    print(f"addr={addr} max|hw-emu|={e_emu:.3e} max|hw-exact|={e_exact:.3e}")
+    assert e_emu < 2e-3
+    assert e_emu <= e_exact
