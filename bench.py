@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark of the helical FDK hot path (rebin -> filter -> backprojection) on B200.
+
+Workload (default, one GPU): the split-precision configuration -- 736 cols x 64 rows at
+0.6 mm, 1152 views/rotation, pitch 0.8, 10 rotations (11,520 views), a seeded phantom of 30
+random ellipsoids (densities 0-2 x mu_water, semi-axes 5-80 mm), Shepp-Logan filter,
+512 x 512 x 256 voxels at 0.5 mm (the first 8 of the 16 blocks the planner allows: the
+reference has no z-range key, MaxBlocks caps it).  Synthetic data: the scan is simulated on the
+GPU (analytic line integrals + Poisson noise, I0 = 1e5).
+
+A step = one full reconstruction of that volume.
+  value  voxel-GUPS = sum over voxels of (a_max - a_min) / step time / 1e9, fan projections
+         resident in HBM (lct_recon_run with device buffers);
+  e2e    the same through lct_recon_run with pinned HOST buffers: H2D of the fan views the
+         volume needs and D2H of the volume inside every timed step.
+Multi-GPU (torchrun): weak scaling, rank r reconstructs blocks [8r, 8r+8) of one longer scan,
+no data-path collective; step time = max over ranks.
+
+`--impl reference` times the reference's formulas on the host CPU (the CPU oracle's FP32
+restatement, every core): the reference has no CPU implementation of the path, so this is a
+port; each step is a bounded sample extrapolated to the whole volume.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+METRIC = "FDK voxel-GUPS & s/volume at relL2<=1e-4 vs FP64 oracle: plain vs mixed+learned"
+UNIT = "voxel-GUPS"
+FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
+
+WORKLOADS = {
+    "cfg2": dict(
+        geo=dict(ns=736, nt=64, ds=0.6, dt=0.6, npt=1152, pitch=0.8, nx=512, ny=512, dx=0.5, dz=0.5),
+        rotations=10, blocks=8, ellipsoids=30, filter_kind=1,
+        label="helical FDK 736x64@0.6mm, 1152 views/rot, pitch 0.8, 10 rot, 30 ellipsoids, "
+              "Shepp-Logan, 512x512x256@0.5mm"),
+    "cfg1": dict(
+        geo=dict(ns=672, nt=16, ds=1.0, dt=1.0, npt=1160, pitch=1.0, nx=256, ny=256, dx=1.0, dz=1.0),
+        rotations=3, blocks=1, ellipsoids=10, filter_kind=0,
+        label="helical FDK 672x16@1mm, 1160 views/rot, pitch 1, >=3.7 rot, Ram-Lak, 256x256x32@1mm"),
+    "cfg5": dict(
+        geo=dict(ns=896, nt=128, ds=0.5, dt=0.5, npt=2304, pitch=1.0, nx=1024, ny=1024, dx=0.4, dz=0.4),
+        rotations=20, blocks=16, ellipsoids=30, filter_kind=1,
+        label="helical FDK 896x128@0.5mm, 2304 views/rot, pitch 1, 20 rot, 1024x1024x512@0.4mm"),
+}
+
+
+# ------------------------------------------------------------------------------------------
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", FALLBACK_HBM_GBS), "measured", d
+    return FALLBACK_HBM_GBS, "fallback", {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.lines: list[str] = []
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", device_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------
+def make_workload(name: str, rank: int, world: int):
+    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.scan import Phantom, ScanGeometry
+
+    w = WORKLOADS[name]
+    geo = ScanGeometry(**w["geo"])
+    geo.readings = int(round(w["rotations"] * geo.npt))
+    need = w["blocks"] * world
+    full = Plan(geo)
+    if full.info.n_blocks < need:  # longer scan for weak scaling / too-short configurations
+        geo = geo.with_blocks(need, cap=False)
+        full = Plan(geo)
+    zlo = full.blocks[0].block_start
+    zhi = full.blocks[need - 1].block_end
+    lo, hi = min(zlo, zhi), max(zlo, zhi)
+    fov = 0.5 * min(geo.nx * geo.dx, geo.ny * geo.dx)
+    ph = Phantom.random(w["ellipsoids"], seed=20240 + w["ellipsoids"], fov_radius=fov,
+                        z_lo=lo, z_hi=hi)
+    geo.max_blocks = w["blocks"]
+    geo.first_block = rank * w["blocks"]
+    params = geo.scan_params()
+    params.first_block = geo.first_block
+    plan = Plan(params=params, angles32=geo.angles32(), zpos32=geo.zpos32())
+    return w, geo, plan, ph
+
+
+def oracle_accuracy(w, geo, plan, fan_block_views, img, interp, rows=2):
+    """rel-L2 / max-abs of slab 0 rows against the FP64 oracle of the same formulas (texture
+    emulation for TEX8) and against the unquantised FP64 oracle."""
+    import oracle as orc
+
+    g, ig = plan.info.ctg, plan.info.ig
+    bi = plan.blocks[plan.info.first_block]
+    h = orc.shepp_logan_taps(g.ns, g.ds) if w["filter_kind"] == 1 else orc.ramp_taps(g.ns, g.ds)
+    betas = plan.angles32[bi.block_proj_start + g.add_projections:][: g.n_angle]
+    y0 = ig.ny // 2 - rows // 2
+    got = img[:32, y0:y0 + rows]
+    out = {}
+    modes = [("same_formulas", orc.TEXEMU if interp == 0 else orc.EXACT)]
+    if interp == 0:
+        modes.append(("fp64_exact", orc.EXACT))
+    for key, m in modes:
+        par = orc.rebin_fan2par(g, fan_block_views, m).astype(np.float32)
+        f = orc.filter_rows(h, par.reshape(-1, g.ns)).reshape(par.shape).astype(np.float32)
+        ref = orc.bp_par(g, ig, betas, f, m, orc.BORDER, rows=(y0, y0 + rows))[:, y0:y0 + rows]
+        out[key] = {"rel_l2": orc.rel_l2(got, ref), "max_abs": orc.max_abs(got, ref)}
+    if interp != 0:
+        out["fp64_exact"] = out["same_formulas"]
+    out["sample"] = f"block {plan.info.first_block}, rows y={y0}..{y0 + rows - 1}, all x, 32 slices"
+    return out
+
+
+def cpu_port_sample(w, geo, plan, fan_block_views, budget_s: float):
+    """The reference's formulas in FP32 on every host core (the oracle's timed restatement):
+    rebin+filter of a sample of views and backprojection of a sample of voxel rows, each
+    extrapolated to the whole volume (the reference's per-block flow: n_blocks * n_angle
+    views rebinned and filtered)."""
+    import oracle as orc
+
+    g, ig = plan.info.ctg, plan.info.ig
+    bi = plan.blocks[plan.info.first_block]
+    h = orc.shepp_logan_taps(g.ns, g.ds) if w["filter_kind"] == 1 else orc.ramp_taps(g.ns, g.ds)
+    betas = plan.angles32[bi.block_proj_start + g.add_projections:][: g.n_angle]
+    threads = orc.lib().orc_num_threads()
+    # calibrate then size each part to about budget/2
+    nv = 8
+    t0 = time.perf_counter()
+    orc.rebin_filter_f32(g, fan_block_views, h, 0, nv)
+    t_view = (time.perf_counter() - t0) / nv
+    nv = int(max(8, min(g.n_angle, budget_s / 2 / max(t_view, 1e-9))))
+    filt = np.zeros((g.n_angle, g.nt, g.ns), dtype=np.float32)
+    t0 = time.perf_counter()
+    filt[:nv] = orc.rebin_filter_f32(g, fan_block_views, h, 0, nv)
+    t_rf = time.perf_counter() - t0
+    t_view = t_rf / nv
+    upd_per_row = 0
+    for z in range(32):
+        a, b = orc.bp_window(g, ig, z)
+        upd_per_row += (b - a) * ig.nx
+    img = np.zeros((ig.nz, ig.ny, ig.nx), dtype=np.float32)
+    t0 = time.perf_counter()
+    orc.bp_par_rows_f32(g, ig, betas, filt, 0, 1, out=img)
+    t_row = time.perf_counter() - t0
+    rows = int(max(1, min(ig.ny, budget_s / 2 / max(t_row, 1e-9))))
+    t0 = time.perf_counter()
+    orc.bp_par_rows_f32(g, ig, betas, filt, 0, rows, out=img)
+    t_bp = time.perf_counter() - t0
+    t_upd = t_bp / (rows * upd_per_row)
+    nb = plan.info.n_blocks_run
+    updates = nb * ig.ny * upd_per_row
+    total = nb * g.n_angle * t_view + updates * t_upd
+    return {
+        "value": updates / total / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+        "sample": f"rebin+filter of {nv} views and backprojection of {rows} of {ig.ny} voxel rows "
+                  f"(x all, 32 slices) of one block, extrapolated to {nb} blocks "
+                  f"({nb * g.n_angle} views rebinned/filtered per block as the reference does); "
+                  f"{t_rf + t_bp:.1f} s of CPU work",
+        "s_per_volume": total,
+    }
+
+
+# ------------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle as orc
+
+    w, geo, plan, ph = make_workload(args.workload, 0, 1)
+    g = plan.info.ctg
+    bi = plan.blocks[0]
+    fan = orc.sim_project(ph.records, geo.ns, geo.nt, geo.ds, geo.dt, np.float32(geo.central_channel),
+                          np.float32((geo.nt - 1) / 2.0), geo.dso, geo.angles64(), geo.zpos64(),
+                          bi.block_proj_start, bi.block_proj_start + g.n_angle_add, 1e5, 7)
+    vals, samples = [], []
+    for i in range(args.warmup + args.steps):
+        r = cpu_port_sample(w, geo, plan, fan, budget_s=args.cpu_budget)
+        if i >= args.warmup:
+            vals.append(r["value"])
+            samples.append(r)
+    v = statistics.median(vals)
+    last = samples[-1]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": last["s_per_volume"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipsoid phantom, simulated scan)",
+        "config": {"workload": w["label"], "volume": [plan.info.n_blocks_run * 32, plan.info.ig.ny, plan.info.ig.nx]},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": last["cores"], "kind": "port",
+                         "sample": last["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    from listctrecons_b200 import capi
+    from listctrecons_b200.recon import Reconstruction
+    from listctrecons_b200.scan import simulate_gpu
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    w, geo, plan, ph = make_workload(args.workload, rank, world)
+    opts = dict(mode=capi.MODE_SCAN if args.mode == "scan" else capi.MODE_BLOCK,
+                filter_kind=w["filter_kind"],
+                filter_mode=capi.FILTER_BF16X3 if args.filter == "bf16x3" else capi.FILTER_FP32,
+                interp=capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT,
+                addr=capi.ADDR_BORDER, bp_nz=args.bp_nz)
+    rec = Reconstruction(plan, **opts)
+    st = rec.stats()
+    f0, fc = rec.fan_first, rec.fan_count
+    log(f"[rank {rank}] views {f0}..{f0 + fc} of {geo.readings}, blocks "
+        f"{plan.info.first_block}..{plan.info.first_block + plan.info.n_blocks_run}")
+    fan = simulate_gpu(geo, ph, i0=1e5, seed=7, v0=f0, v1=f0 + fc)
+    img = torch.empty(rec.image_shape, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def maxr(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        rec.run(fan, img, fan_view0=f0)
+    torch.cuda.synchronize()
+
+    props = torch.cuda.get_device_properties(dev)
+    uuid = str(getattr(props, "uuid", "")) if hasattr(props, "uuid") else ""
+    dev_id = ("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or str(dev.index))
+    clocks = ClockSampler(dev_id)
+    time.sleep(0.3)
+
+    # device-resident timed region
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    bp_ms, stage = [], []
+    e0.record(stream)
+    for _ in range(args.steps):
+        rec.run(fan, img, fan_view0=f0)
+        t = rec.last_times()
+        stage.append(t)
+        bp_ms.append(t["backproject"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms = maxr(e0.elapsed_time(e1) / args.steps)
+    launches = rec.stats().launches * args.steps
+
+    # end to end through the C ABI with pinned host buffers
+    h_fan = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
+    h_fan.copy_(fan)
+    h_img = torch.empty(rec.image_shape, dtype=torch.float32, pin_memory=True)
+    for _ in range(max(1, args.warmup)):
+        rec.run(h_fan, h_img, fan_view0=f0)
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        rec.run(h_fan, h_img, fan_view0=f0)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = maxr(e2.elapsed_time(e3) / args.steps)
+    launches += rec.stats().launches * args.steps
+    clk = clocks.stop()
+
+    updates_all = st.voxel_updates * world
+    value = updates_all / (ms / 1e3) / 1e9
+    e2e = updates_all / (e2e_ms / 1e3) / 1e9
+    if rank != 0:
+        return 0
+
+    # roofline of the dominant kernel (backprojection), from its in-library event timing
+    g, ig = plan.info.ctg, plan.info.ig
+    nb = plan.info.n_blocks_run
+    bp = statistics.mean(bp_ms)
+    alg_bytes = nb * g.n_angle * g.nt * g.ns * 4 + nb * 32 * ig.nx * ig.ny * 4
+    peak, peak_kind, peaks = measured_peaks()
+    achieved = alg_bytes / (bp / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(f"{args.workload}:{args.mode}:{args.interp}")
+    sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    l1_peak = 128.0 * props.multi_processor_count * sm_mhz * 1e6 / 1e9  # GB/s, 128 B/clk/SM
+    l1_achieved = st.voxel_updates * 32 / (bp / 1e3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 30-ellipsoid phantom, analytic helical scan + Poisson I0=1e5, simulated on the GPU)",
+        "config": {"workload": w["label"], "volume": [nb * 32, ig.ny, ig.nx],
+                   "views_read": fc, "mode": args.mode, "interp": args.interp,
+                   "filter": args.filter, "bp_nz": args.bp_nz or "auto",
+                   "l2": "inputs larger than L2 (fan %.2f GB, filtered views %.2f GB)" % (
+                       fc * g.nt * g.ns * 4 / 1e9, st.rebinned_views * g.nt * g.ns * 4 / 1e9),
+                   "parallelism": f"slab shards x{world}"},
+        "s_per_volume": ms / 1e3,
+        "stages_ms": {k: statistics.mean(t[k] for t in stage) for k in stage[0]},
+        "e2e": {"value": e2e, "unit": UNIT, "s_per_volume": e2e_ms / 1e3,
+                "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
+        "gpu_launches": launches,
+        "roofline": {"kernel": "bp_par_pairs_kernel", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes": alg_bytes, "launch_ms": bp},
+        "roofline_onchip": {"bound": "l1", "achieved": l1_achieved, "peak": l1_peak, "unit": "GB/s",
+                            "frac": l1_achieved / l1_peak,
+                            "note": "32 B per voxel-view update (8 FP32 taps) vs 128 B/clk/SM nominal "
+                                    "at the median SM clock"},
+        "clocks": clk,
+    }
+    if not args.no_accuracy:
+        bi = plan.blocks[plan.info.first_block]
+        lo = bi.block_proj_start - f0
+        fb = fan[lo: lo + g.n_angle_add].cpu().numpy()
+        line["accuracy"] = oracle_accuracy(w, geo, plan, fb, img.cpu().numpy(), opts["interp"])
+    if not args.no_cpu and world == 1:
+        bi = plan.blocks[plan.info.first_block]
+        lo = bi.block_proj_start - f0
+        fb = fan[lo: lo + g.n_angle_add].cpu().numpy()
+        line["cpu_baseline"] = {k: v for k, v in cpu_port_sample(w, geo, plan, fb, args.cpu_budget).items()
+                                if k != "s_per_volume"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", default="scan", choices=["scan", "block"])
+    ap.add_argument("--filter", default="fp32", choices=["fp32", "bf16x3"])
+    ap.add_argument("--interp", default="exact", choices=["tex8", "exact"],
+                    help="exact: FP64 geometry, full FP32 weights (the FP64-oracle accuracy bar); "
+                         "tex8: the reference's texture sampling (drop-in parity)")
+    ap.add_argument("--bp-nz", type=int, default=0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    else:
+        torch.cuda.set_device(0)
+    try:
+        return run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

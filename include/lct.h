@@ -163,7 +163,8 @@ typedef struct lct_scan_params {
   float r_src_to_iso;
   float central_channel;
   int n_proj_turn;
-  int max_blocks; /* new optional key MaxBlocks: reconstruct only the first N blocks (0 = all) */
+  int max_blocks;  /* new optional key MaxBlocks: reconstruct at most N blocks (0 = all) */
+  int first_block; /* new optional key FirstBlock: start at this block (0 = the first) */
 } lct_scan_params;
 
 typedef struct lct_plan_info {
@@ -174,7 +175,8 @@ typedef struct lct_plan_info {
   float data_begin_pos, data_end_pos, allow_begin, allow_end, start_pos, end_pos;
   float recon_start_pos, recon_end_pos;
   int n_slices_recon, n_slices_block, n_blocks, data_offset;
-  int n_blocks_run; /* min(n_blocks, max_blocks) */
+  int first_block;  /* first block reconstructed */
+  int n_blocks_run; /* blocks reconstructed: min(n_blocks - first_block, max_blocks) */
 } lct_plan_info;
 
 /* BlockInfo (Include/DataStructs.h:281-311) of one block. */
@@ -231,14 +233,26 @@ typedef struct lct_recon lct_recon;
 
 /* Allocates every device buffer the plan needs (no allocation happens in run). */
 int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out);
-/* Reconstructs n_blocks_run blocks.  fan: all `readings` views [readings][nt][ns] float
-   (host: pinned or pageable; device: a device pointer); image: [n_blocks_run*32][ny][nx]. */
-int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, float* image,
-                  int image_on_device, lct_stream stream);
+/* Reconstructs blocks [first_block, first_block + n_blocks_run).  fan: [views][nt][ns] float
+   holding fan views from `fan_view0` on (file view numbering, DataOffset included) and at
+   least through the run's range (lct_recon_fan_range); host (pinned or pageable) or device.
+   image: [n_blocks_run*32][ny][nx].  Returns after the image is complete (synchronous). */
+int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
+                  float* image, int image_on_device, lct_stream stream);
 /* Device-side per-stage time of the last run (ms): h2d, rebin, filter, backproject, d2h. */
 int lct_recon_last_times(const lct_recon* r, float* ms5);
 /* Fan views [first, first+count) the run reads (h2d bytes = count*nt*ns*4). */
 int lct_recon_fan_range(const lct_recon* r, int64_t* first, int64_t* count);
+
+typedef struct lct_recon_stats {
+  int64_t voxel_updates;  /* sum over reconstructed voxels of (a_max - a_min): iterations of
+                             CUDA/Backprojector.cu:46 the reference would run */
+  int64_t h2d_bytes;      /* fan bytes a host-buffer run copies in */
+  int64_t d2h_bytes;      /* image bytes a host-buffer run copies out */
+  int64_t rebinned_views; /* parallel views rebinned and filtered per run */
+  int launches;           /* kernels launched by the last run */
+} lct_recon_stats;
+int lct_recon_stats_get(const lct_recon* r, lct_recon_stats* out);
 void lct_recon_destroy(lct_recon* r);
 
 /* ---------------------------------------------------------------------------------------

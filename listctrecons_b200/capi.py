@@ -71,7 +71,7 @@ class ScanParams(C.Structure):
         ("dx", C.c_float), ("dz", C.c_float), ("offset_x", C.c_float), ("offset_y", C.c_float),
         ("readings", C.c_int), ("view_offset", C.c_int), ("data_offset", C.c_int),
         ("r_src_to_iso", C.c_float), ("central_channel", C.c_float),
-        ("n_proj_turn", C.c_int), ("max_blocks", C.c_int),
+        ("n_proj_turn", C.c_int), ("max_blocks", C.c_int), ("first_block", C.c_int),
     ]
 
 
@@ -84,7 +84,7 @@ class PlanInfo(C.Structure):
         ("start_pos", C.c_float), ("end_pos", C.c_float),
         ("recon_start_pos", C.c_float), ("recon_end_pos", C.c_float),
         ("n_slices_recon", C.c_int), ("n_slices_block", C.c_int), ("n_blocks", C.c_int),
-        ("data_offset", C.c_int), ("n_blocks_run", C.c_int),
+        ("data_offset", C.c_int), ("first_block", C.c_int), ("n_blocks_run", C.c_int),
     ]
 
 
@@ -93,6 +93,13 @@ class BlockInfo(C.Structure):
         ("block_idx", C.c_int), ("block_proj_start", C.c_int), ("block_proj_end", C.c_int),
         ("block_start", C.c_float), ("block_end", C.c_float),
         ("block_slice_start", C.c_int), ("block_slice_end", C.c_int),
+    ]
+
+
+class ReconStats(C.Structure):
+    _fields_ = [
+        ("voxel_updates", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+        ("rebinned_views", C.c_int64), ("launches", C.c_int),
     ]
 
 
@@ -134,9 +141,10 @@ SIGNATURES: dict[str, tuple] = {
     "lct_plan_destroy": (None, [P]),
     "lct_recon_opts_default": (None, [C.POINTER(ReconOpts)]),
     "lct_recon_create": (I32, [P, C.POINTER(ReconOpts), C.POINTER(P)]),
-    "lct_recon_run": (I32, [P, P, I32, P, I32, P]),
+    "lct_recon_run": (I32, [P, P, I64, I32, P, I32, P]),
     "lct_recon_last_times": (I32, [P, P]),
     "lct_recon_fan_range": (I32, [P, C.POINTER(I64), C.POINTER(I64)]),
+    "lct_recon_stats_get": (I32, [P, C.POINTER(ReconStats)]),
     "lct_recon_destroy": (None, [P]),
     "lct_sim_project": (I32, [P, I32, I32, I32, F32, F32, F32, F32, F32, P, P, I64, I64, F64, U64, P, P]),
     "lct_diag_tex3d_sample": (I32, [P, I32, I32, I32, P, I64, I32, P]),

@@ -93,6 +93,11 @@ __device__ __forceinline__ float sample_rows(const float* __restrict__ view, int
   const float v01 = (rk0 && c.ok1) ? __ldg(p0 + c.c1) : 0.0f;
   const float v10 = (rk1 && c.ok0) ? __ldg(p1 + c.c0) : 0.0f;
   const float v11 = (rk1 && c.ok1) ? __ldg(p1 + c.c1) : 0.0f;
+  if (INTERP == LCT_INTERP_TEX8) {
+    float w00, w01, w10, w11;
+    tex_bilinear_weights(c.a, b, w00, w01, w10, w11);
+    return fmaf(w11, v11, fmaf(w10, v10, fmaf(w01, v01, w00 * v00)));
+  }
   const float top = fmaf(c.a, v01, (1.0f - c.a) * v00);
   const float bot = fmaf(c.a, v11, (1.0f - c.a) * v10);
   return fmaf(b, bot, (1.0f - b) * top);

@@ -10,7 +10,7 @@
 //     Src/DataStructs.cpp:17,22,27; results are identical whenever its read is in bounds);
 //   * sizes are 64-bit and a block whose view window leaves the data is rejected (the
 //     reference reads outside the file there, Src/DataReader.cpp:14);
-//   * the optional MaxBlocks key caps the number of blocks reconstructed.
+//   * the optional MaxBlocks / FirstBlock keys select the blocks reconstructed.
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -171,7 +171,10 @@ static int plan_build(lct_plan& P) {
   I.n_slices_block = nsb;
   I.n_blocks = n_blocks;
   I.data_offset = fp.data_offset;
-  I.n_blocks_run = (fp.max_blocks > 0 && fp.max_blocks < n_blocks) ? fp.max_blocks : n_blocks;
+  if (fp.first_block < 0 || (fp.first_block > 0 && fp.first_block >= n_blocks)) return LCT_ERR_RANGE;
+  I.first_block = fp.first_block;
+  const int left = n_blocks - fp.first_block;
+  I.n_blocks_run = (fp.max_blocks > 0 && fp.max_blocks < left) ? fp.max_blocks : left;
 
   P.blocks.clear();
   lct_block_info b0;

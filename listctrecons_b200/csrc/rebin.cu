@@ -158,6 +158,17 @@ __device__ __forceinline__ float tex3d_lin(const float* __restrict__ v, int nx, 
   lin_axis<INTERP>(x, i, a);
   lin_axis<INTERP>(y, j, b);
   lin_axis<INTERP>(z, k, c);
+  // (x, y) corner weights: the texture unit's rule for TEX8 (exact products otherwise); the
+  // slices are then combined with the z weight
+  float wxy[2][2];
+  if (INTERP == LCT_INTERP_TEX8) {
+    tex_bilinear_weights(a, b, wxy[0][0], wxy[0][1], wxy[1][0], wxy[1][1]);
+  } else {
+    wxy[0][0] = (1.0f - a) * (1.0f - b);
+    wxy[0][1] = a * (1.0f - b);
+    wxy[1][0] = (1.0f - a) * b;
+    wxy[1][1] = a * b;
+  }
   float s = 0.0f;
 #pragma unroll
   for (int dk = 0; dk < 2; ++dk)
@@ -166,7 +177,7 @@ __device__ __forceinline__ float tex3d_lin(const float* __restrict__ v, int nx, 
 #pragma unroll
       for (int di = 0; di < 2; ++di) {
         int ii = i + di, jj = j + dj, kk = k + dk;
-        float wgt = (di ? a : 1.0f - a) * (dj ? b : 1.0f - b) * (dk ? c : 1.0f - c);
+        float wgt = wxy[dj][di] * (dk ? c : 1.0f - c);
         if (ADDR == LCT_ADDR_CLAMP) {
           ii = min(max(ii, 0), nx - 1);
           jj = min(max(jj, 0), ny - 1);

@@ -38,6 +38,8 @@ struct lct_recon {
   cudaEvent_t ev[6] = {};
   float times[5] = {};
   int device = 0;
+  long long voxel_updates = 0;
+  int launches = 0;
 };
 
 namespace lct {
@@ -60,6 +62,9 @@ static int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
   const double act = 0.5 * (double)g.pitch / (double)ig.dz;
   return act >= 20.0 ? 16 : 8;
 }
+
+// kernels one filter call launches
+static int filter_launches(int mode) { return mode == LCT_FILTER_BF16X3 ? 2 : 1; }
 
 static int block_addr(const lct_recon* r, int b) {
   if (r->o.addr == LCT_ADDR_LEGACY) return b == 0 ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
@@ -113,7 +118,7 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
   }
   for (int b = 0; b < nb; ++b) {
     lct_block_info bi;
-    lct_plan_block(plan, b, &bi);
+    lct_plan_block(plan, r->info.first_block + b, &bi);
     r->blocks.push_back(bi);
   }
   r->plane = (long long)g.nt * g.ns;
@@ -134,6 +139,16 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
   r->g_first = lo + g.add_projections;
   r->g_count = r->fan_count - 2LL * g.add_projections;
   cudaGetDevice(&r->device);
+  {
+    // sum of the reference's per-voxel view counts (same windows in every block)
+    const float dzv = g.pitch / (float)g.n_proj_turn;
+    long long per_block = 0;
+    for (int z = 0; z < kBlockSlices; ++z) {
+      BpWindow w = bp_window(g, r->info.ig, z, dzv, g.n_proj_turn / 2);
+      per_block += (long long)(w.a_max - w.a_min) * r->info.ig.nx * r->info.ig.ny;
+    }
+    r->voxel_updates = per_block * nb;
+  }
 
   int st = LCT_OK;
   const long long par_views = o.mode == LCT_MODE_SCAN ? r->g_count : g.n_angle;
@@ -170,6 +185,18 @@ LCT_API int lct_recon_fan_range(const lct_recon* r, int64_t* first, int64_t* cou
   return LCT_OK;
 }
 
+LCT_API int lct_recon_stats_get(const lct_recon* r, lct_recon_stats* out) {
+  if (!r || !out) return LCT_ERR_ARG;
+  out->voxel_updates = r->voxel_updates;
+  out->h2d_bytes = r->fan_count * r->plane * (long long)sizeof(float);
+  out->d2h_bytes = (long long)r->info.n_blocks_run * kBlockSlices * r->info.ig.nx * r->info.ig.ny *
+                   (long long)sizeof(float);
+  out->rebinned_views = r->o.mode == LCT_MODE_SCAN ? r->g_count
+                                                   : (long long)r->info.n_blocks_run * r->info.ctg.n_angle;
+  out->launches = r->launches;
+  return LCT_OK;
+}
+
 LCT_API int lct_recon_last_times(const lct_recon* r, float* ms5) {
   if (!r || !ms5) return LCT_ERR_ARG;
   std::memcpy(ms5, r->times, sizeof(r->times));
@@ -186,23 +213,26 @@ static int run_rebin(lct_recon* r, const lct_geom& g, const float* fan_block, fl
   }
 }
 
-LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, float* image,
-                          int image_on_device, lct_stream stream) {
+LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
+                          float* image, int image_on_device, lct_stream stream) {
   if (!r || !fan || !image) return LCT_ERR_ARG;
+  if (fan_view0 < 0 || fan_view0 > r->fan_first + r->info.data_offset) return LCT_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   const lct_geom& g = r->info.ctg;
   const lct_img& ig = r->info.ig;
   const int nb = r->info.n_blocks_run;
   const long long off = r->info.data_offset;
   int st;
+  r->launches = 0;
   if ((st = cuda_status(cudaEventRecord(r->ev[0], s)))) return st;
 
   // fan views needed by the run (the union of the blocks' windows)
   const float* d_fan;
+  const long long skip = r->fan_first + off - fan_view0;  // views before the run's first
   if (fan_on_device) {
-    d_fan = fan + (r->fan_first + off) * r->plane;
+    d_fan = fan + skip * r->plane;
   } else {
-    if ((st = cuda_status(cudaMemcpyAsync(r->d_fan, fan + (r->fan_first + off) * r->plane,
+    if ((st = cuda_status(cudaMemcpyAsync(r->d_fan, fan + skip * r->plane,
                                           sizeof(float) * r->fan_count * r->plane,
                                           cudaMemcpyHostToDevice, s))))
       return st;
@@ -222,10 +252,15 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, flo
       const int addr = block_addr(r, b);
       const float* fan_block = d_fan + (bi.block_proj_start - r->fan_first) * r->plane;
       if ((st = run_rebin(r, g, fan_block, r->d_par, addr, s))) return st;
-      if (r->o.preweight == LCT_PW_PI_ORI && (st = lct_weight_pi_ori(&g, r->d_par, s))) return st;
+      r->launches++;
+      if (r->o.preweight == LCT_PW_PI_ORI) {
+        if ((st = lct_weight_pi_ori(&g, r->d_par, s))) return st;
+        r->launches++;
+      }
       if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, (long long)g.n_angle * g.nt,
                                    r->o.filter_mode, s)))
         return st;
+      r->launches += filter_launches(r->o.filter_mode);
       const float* betas = r->d_betas + bi.block_proj_start + g.add_projections;
       float* img_b = d_img + (long long)b * slab;
       if (r->o.backprojector == LCT_BP_PI_ORI) {
@@ -247,6 +282,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, flo
         st = launch_bp_par(g, ig, L, s);
       }
       if (st) return st;
+      r->launches++;
     }
     cudaEventRecord(r->ev[4], s);
   } else {
@@ -263,15 +299,18 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, flo
                                           r->g_count, r->o.interp, addr0, s)))
         return st;
     }
+    r->launches++;
     if (r->o.preweight == LCT_PW_PI_ORI) {
       lct_geom gg = g;
       gg.n_angle = (int)r->g_count;
       gg.n_angle_add = (int)r->g_count;
       if ((st = lct_weight_pi_ori(&gg, r->d_par, s))) return st;
+      r->launches++;
     }
     if ((st = cuda_status(cudaEventRecord(r->ev[2], s)))) return st;
     if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, r->g_count * g.nt, r->o.filter_mode, s)))
       return st;
+    r->launches += filter_launches(r->o.filter_mode);
     if ((st = cuda_status(cudaEventRecord(r->ev[3], s)))) return st;
     if (r->o.backprojector == LCT_BP_PI_ORI) {
       for (int b = 0; b < nb; ++b) {
@@ -279,6 +318,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, flo
         st = lct_backproject_pi_ori(&g, &ig, r->d_betas + gv, r->d_par + (gv - r->g_first) * r->plane,
                                     d_img + (long long)b * slab, r->o.interp, block_addr(r, b), s);
         if (st) return st;
+        r->launches++;
       }
     } else {
       // one launch over every slab; with LEGACY addressing slab 0 runs apart (clamped)
@@ -306,6 +346,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int fan_on_device, flo
         // betas are indexed by the same slab offset: shift the base by g_first
         L.betas = r->d_betas + r->g_first;
         if ((st = launch_bp_par(g, ig, L, s))) return st;
+        r->launches++;
         b0 = b1;
       }
     }

@@ -10,10 +10,23 @@
 
 namespace lct {
 
-// 8-fractional-bit weight (round to nearest, ties up).  The texture-hardware GPU test pins
-// this rule against cudaFilterModeLinear samples.
+// 8-fractional-bit weight (round to nearest, ties up), as measured on the texture unit.
 __host__ __device__ __forceinline__ float q8(float a) {
   return floorf(a * 256.0f + 0.5f) * (1.0f / 256.0f);
+}
+
+// Bilinear corner weights of the texture unit, measured on B200 (tests/test_gpu_texture.py,
+// fixture tests/golden/tex_hw.npz): with a = q8(frac x) and b = q8(frac y), the far corner
+// gets w11 = round-half-up(a*b) on the 1/256 grid and the others follow by subtraction, so each
+// axis keeps its weight exactly: w01 = a - w11, w10 = b - w11, w00 = 1 - a - b + w11.
+// Every product and difference here is exact in FP32 (multiples of 2^-16).
+__host__ __device__ __forceinline__ void tex_bilinear_weights(float a, float b, float& w00,
+                                                              float& w01, float& w10,
+                                                              float& w11) {
+  w11 = floorf(a * b * 256.0f + 0.5f) * (1.0f / 256.0f);
+  w01 = a - w11;
+  w10 = b - w11;
+  w00 = (1.0f - a - b) + w11;
 }
 
 template <int INTERP>

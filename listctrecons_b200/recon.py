@@ -109,19 +109,25 @@ class Reconstruction:
         info = plan.info
         self.image_shape = (info.n_blocks_run * BLOCK_SLICES, info.ig.ny, info.ig.nx)
 
-    def run(self, fan, image=None, stream=None):
-        """fan: CUDA tensor or host tensor/array [readings][nt][ns] float32 (host memory is
-        copied inside; pinned is fastest); image: same side as wanted, or None (a CUDA tensor
-        is allocated)."""
+    def run(self, fan, image=None, stream=None, fan_view0: int = 0):
+        """fan: CUDA tensor or host tensor/array [views][nt][ns] float32 holding fan views from
+        `fan_view0` on (all readings by default; at least [fan_first, fan_first+fan_count));
+        host memory is copied inside, pinned is fastest.  image: same side as wanted, or None
+        (a CUDA tensor is allocated)."""
         torch = _torch()
         if image is None:
             image = torch.empty(self.image_shape, dtype=torch.float32, device="cuda")
         f_dev, f_ptr = _ptr(fan)
         i_dev, i_ptr = _ptr(image)
         s = stream if stream is not None else _stream()
-        capi.check(self._lib.lct_recon_run(self._h, f_ptr, int(f_dev), i_ptr, int(i_dev), s),
-                   "lct_recon_run")
+        capi.check(self._lib.lct_recon_run(self._h, f_ptr, int(fan_view0), int(f_dev), i_ptr,
+                                           int(i_dev), s), "lct_recon_run")
         return image
+
+    def stats(self) -> capi.ReconStats:
+        st = capi.ReconStats()
+        capi.check(self._lib.lct_recon_stats_get(self._h, C.byref(st)))
+        return st
 
     def last_times(self) -> dict:
         t = (C.c_float * 5)()

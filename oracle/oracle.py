@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
             "orc_rebin_pi_ori": (None, [G, P, P, C.c_int, C.c_int]),
             "orc_weight_pi_ori": (None, [G, P]),
             "orc_ramp_taps": (None, [C.c_int, C.c_float, P]),
+            "orc_shepp_logan_taps": (None, [C.c_int, C.c_float, P]),
             "orc_filter_rows": (None, [P, C.c_int, P, P, C.c_long, C.c_int]),
             "orc_bp_window": (None, [G, Ip, C.c_int, C.c_float, C.c_int, P, P]),
             "orc_bp_par_rows": (None, [G, Ip, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
@@ -156,6 +157,12 @@ def weight_pi_ori(g, proj):
 def ramp_taps(ns, ds):
     h = np.zeros(2 * ns, dtype=np.float32)
     lib().orc_ramp_taps(ns, ds, h.ctypes.data)
+    return h
+
+
+def shepp_logan_taps(ns, ds):
+    h = np.zeros(2 * ns, dtype=np.float32)
+    lib().orc_shepp_logan_taps(ns, ds, h.ctypes.data)
     return h
 
 
