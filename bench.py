@@ -124,11 +124,14 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------
-def make_workload(name: str, rank: int, world: int):
+def make_workload(name: str, rank: int, world: int, blocks: int = 0):
     from listctrecons_b200.recon import Plan
     from listctrecons_b200.scan import Phantom, ScanGeometry
 
-    w = WORKLOADS[name]
+    w = dict(WORKLOADS[name])
+    if blocks:
+        w["blocks"] = blocks
+        w["label"] = w["label"] + f" (first {blocks} blocks)"
     geo = ScanGeometry(**w["geo"])
     geo.readings = int(round(w["rotations"] * geo.npt))
     need = w["blocks"] * world
@@ -267,12 +270,12 @@ def run_ours(args, rank, world, dist):
     from listctrecons_b200.scan import simulate_gpu
 
     dev = torch.device("cuda", torch.cuda.current_device())
-    w, geo, plan, ph = make_workload(args.workload, rank, world)
+    w, geo, plan, ph = make_workload(args.workload, rank, world, args.blocks)
     opts = dict(mode=capi.MODE_SCAN if args.mode == "scan" else capi.MODE_BLOCK,
                 filter_kind=w["filter_kind"],
                 filter_mode=capi.FILTER_BF16X3 if args.filter == "bf16x3" else capi.FILTER_FP32,
                 interp=capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT,
-                addr=capi.ADDR_BORDER, bp_nz=args.bp_nz)
+                addr=capi.ADDR_BORDER, bp_nz=args.bp_nz, bp_minb=args.bp_minb)
     rec = Reconstruction(plan, **opts)
     st = rec.stats()
     f0, fc = rec.fan_first, rec.fan_count
@@ -367,7 +370,7 @@ def run_ours(args, rank, world, dist):
         "data": "synthetic (seeded 30-ellipsoid phantom, analytic helical scan + Poisson I0=1e5, simulated on the GPU)",
         "config": {"workload": w["label"], "volume": [nb * 32, ig.ny, ig.nx],
                    "views_read": fc, "mode": args.mode, "interp": args.interp,
-                   "filter": args.filter, "bp_nz": args.bp_nz or "auto",
+                   "filter": args.filter, "bp_nz": args.bp_nz or "auto", "bp_minb": args.bp_minb or "auto",
                    "l2": "inputs larger than L2 (fan %.2f GB, filtered views %.2f GB)" % (
                        fc * g.nt * g.ns * 4 / 1e9, st.rebinned_views * g.nt * g.ns * 4 / 1e9),
                    "parallelism": f"slab shards x{world}"},
@@ -414,6 +417,8 @@ def main() -> int:
                     help="exact: FP64 geometry, full FP32 weights (the FP64-oracle accuracy bar); "
                          "tex8: the reference's texture sampling (drop-in parity)")
     ap.add_argument("--bp-nz", type=int, default=0)
+    ap.add_argument("--bp-minb", type=int, default=0)
+    ap.add_argument("--blocks", type=int, default=0, help="override the blocks per GPU (profiling)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

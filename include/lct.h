@@ -224,7 +224,8 @@ typedef struct lct_recon_opts {
   int backprojector; /* LCT_BP_* */
   int interp;        /* LCT_INTERP_* */
   int addr;          /* LCT_ADDR_* */
-  int bp_nz;         /* backprojection slices per thread (0 = tuned) */
+  int bp_nz;         /* backprojection slices per thread: 4, 8, 16 (0 = tuned) */
+  int bp_minb;       /* backprojection CTAs per SM the register budget targets: 1-4 (0 = tuned) */
 } lct_recon_opts;
 
 void lct_recon_opts_default(lct_recon_opts* o);

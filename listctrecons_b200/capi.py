@@ -108,6 +108,7 @@ class ReconOpts(C.Structure):
         ("mode", C.c_int), ("rebinner", C.c_int), ("preweight", C.c_int),
         ("filter_kind", C.c_int), ("window", C.c_int), ("filter_mode", C.c_int),
         ("backprojector", C.c_int), ("interp", C.c_int), ("addr", C.c_int), ("bp_nz", C.c_int),
+        ("bp_minb", C.c_int),
     ]
 
 

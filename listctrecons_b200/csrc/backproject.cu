@@ -103,10 +103,12 @@ __device__ __forceinline__ float sample_rows(const float* __restrict__ view, int
   return fmaf(b, bot, (1.0f - b) * top);
 }
 
+// cos/sin of a view angle in FP64, rounded to float.  sincospi needs no large-argument
+// reduction (no slow-path call), and beta / pi is exact to double rounding.
 __device__ __forceinline__ void view_trig(const float* __restrict__ betas, int v, float& c,
                                           float& s) {
   double sd, cd;
-  sincos((double)__ldg(betas + v), &sd, &cd);
+  sincospi((double)__ldg(betas + v) * 0.31830988618379067154, &sd, &cd);
   c = (float)cd;
   s = (float)sd;
 }
@@ -505,6 +507,33 @@ LCT_API int lct_backproject_par(const lct_geom* g, const lct_img* ig, const floa
   if (interp != LCT_INTERP_TEX8 && interp != LCT_INTERP_EXACT) return LCT_ERR_ARG;
   if (addr != LCT_ADDR_BORDER && addr != LCT_ADDR_CLAMP) return LCT_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
+  // Full windows (every reference block): pack the views into quad layout in stream-ordered
+  // scratch (n_angle * (nt + 3) * (ns + 3) * 16 bytes, released on the stream) and run the
+  // quad kernel.
+  if (ig->nz <= kBpMaxZ && bp_windows_full(*g, *ig, ig->nz)) {
+    float4* q = nullptr;
+    const size_t bytes = sizeof(float4) * (size_t)g->n_angle * quad_view_elems(g->ns, g->nt);
+    if ((st = cuda_status(cudaMallocAsync((void**)&q, bytes, s)))) return LCT_ERR_ALLOC;
+    st = launch_quad_pack(d_proj, g->n_angle, g->ns, g->nt, addr, q, s);
+    if (!st) {
+      BpLaunch L;
+      L.proj = d_proj;
+      L.betas = d_betas;
+      L.img = d_img;
+      L.view_stride = (long long)g->nt * g->ns;
+      L.n_angle = g->n_angle;
+      L.nz = ig->nz;
+      L.n_slabs = 1;
+      L.slab_view[0] = 0;
+      L.slab_z0[0] = 0;
+      L.interp = interp;
+      L.addr = addr;
+      L.nz_thread = 8;
+      st = launch_bp_par_quads(*g, *ig, L, q, s);
+    }
+    int st2 = cuda_status(cudaFreeAsync(q, s));
+    return st ? st : st2;
+  }
   // slices in chunks of 32 (each chunk has its own window table; the voxel z coordinate is
   // the slice index of the whole image, as in the reference)
   for (int zb = 0; zb < ig->nz; zb += kBpMaxZ) {

@@ -1,0 +1,329 @@
+// Stage 4, fast path: backprojection from filtered views packed in quad layout.
+//
+// Same algorithm and window logic as bp_par_pairs_kernel (backproject.cu): one thread per
+// (x, y) voxel column of NZ slices, z-invariant terms once per view, each conjugate pair
+// {ia, ia + half} of a full window evaluated once and doubled (both samples outside the rows:
+// each added once).  What changes is the per-sample cost:
+//   * a bilinear sample is ONE 16-byte load of the 2 x 2 texel block at the clamped sample
+//     origin (quad layout, lct_internal.h); border/clamp addressing lives in the packed data,
+//     so there are no per-texel bounds tests;
+//   * the row coordinate of slice j is one FMA, qhat = zc[j] * k + m, with k and m per view;
+//   * the pair weights are branch-free selects around one reciprocal;
+//   * views whose window covers every slice of the thread's chunk run an unpredicated loop.
+// EXACT keeps FP64 view trigonometry and full FP32 weights; TEX8 keeps the reference's order
+// for the sample column (phat/dso, theta*dso/ds) and the texture unit's 8-bit weight rules.
+#include <climits>
+#include <cmath>
+
+#include "lct_internal.h"
+#include "tex_emul.cuh"
+
+namespace lct {
+
+constexpr int kQTX = 32, kQTY = 8, kQVB = 32;
+
+// cos/sin of a view angle in FP64 rounded to float (sincospi: no large-argument reduction)
+__device__ __forceinline__ void view_trig_pi(const float* __restrict__ betas, int v, float& c,
+                                             float& s) {
+  double sd, cd;
+  sincospi((double)__ldg(betas + v) * 0.31830988618379067154, &sd, &cd);
+  c = (float)cd;
+  s = (float)sd;
+}
+
+struct BpQuadArgs {
+  const float4* quads;  // view 0 of slab 0's local view 0 is quads + slab_view[s] * qstride
+  const float* betas;
+  float* img;
+  long long qstride;    // float4 per view
+  int qcols;            // ns + 3
+  int ns, nt, n_angle, nx, ny, nz;
+  float ws, wt, ds, dso, dso2, inv_dso, dso_over_ds, orbit, inv_orbit, z0, dzv, kq;
+  float wx, wy, wz, dx, dy, dz;
+  int half;
+  int zchunks;
+  int slab_view[kBpMaxSlabs];
+  int slab_z0[kBpMaxSlabs];
+  int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
+};
+
+// quad pack: grid (views, nt + 3), block 256 over the ns + 3 quad columns
+template <int ADDR>
+__global__ void __launch_bounds__(256) quad_pack_kernel(const float* __restrict__ rows, int ns,
+                                                        int nt, float4* __restrict__ quads) {
+  const long long v = blockIdx.x;
+  const int j = (int)blockIdx.y - 2;
+  const float* view = rows + v * (long long)nt * ns;
+  float4* out = quads + v * quad_view_elems(ns, nt) + (long long)blockIdx.y * quad_cols(ns);
+  auto texel = [&](int r, int c) -> float {
+    if (ADDR == LCT_ADDR_CLAMP) {
+      r = min(max(r, 0), nt - 1);
+      c = min(max(c, 0), ns - 1);
+    } else if (r < 0 || r >= nt || c < 0 || c >= ns) {
+      return 0.0f;
+    }
+    return __ldg(view + (long long)r * ns + c);
+  };
+  for (int q = threadIdx.x; q < ns + 3; q += blockDim.x) {
+    const int i = q - 2;
+    out[q] = make_float4(texel(j, i), texel(j, i + 1), texel(j + 1, i), texel(j + 1, i + 1));
+  }
+}
+
+int launch_quad_pack(const float* rows, long long views, int ns, int nt, int addr, float4* quads,
+                     cudaStream_t s) {
+  if (views <= 0) return LCT_OK;
+  if (views > 0x7fffffffLL || nt + 3 > 65535) return LCT_ERR_ARG;
+  dim3 grid((unsigned)views, nt + 3);
+  if (addr == LCT_ADDR_CLAMP)
+    quad_pack_kernel<LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(rows, ns, nt, quads);
+  else
+    quad_pack_kernel<LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(rows, ns, nt, quads);
+  return launch_status();
+}
+
+// Bilinear sample at origin column already applied to qb (qb = view base + clamped column);
+// q_idx is the row coordinate in texel units (texel centres at integers).
+template <int INTERP>
+__device__ __forceinline__ float quad_sample(const float4* __restrict__ qb, int qcols, int nt,
+                                             float a, float q_idx) {
+  float yb;
+  if (INTERP == LCT_INTERP_TEX8)
+    yb = __fsub_rn(__fadd_rn(q_idx, 0.5f), 0.5f);  // the reference's texture coordinate
+  else
+    yb = q_idx;
+  const float fy = floorf(yb);
+  float b = yb - fy;
+  int j = (int)fy;
+  j = min(max(j, -2), nt);
+  const float4 v = __ldg(qb + (j + 2) * qcols);
+  if (INTERP == LCT_INTERP_TEX8) {
+    b = q8(b);
+    float w00, w01, w10, w11;
+    tex_bilinear_weights(a, b, w00, w01, w10, w11);
+    return fmaf(w11, v.w, fmaf(w10, v.z, fmaf(w01, v.y, w00 * v.x)));
+  }
+  const float top = fmaf(a, v.y - v.x, v.x);
+  const float bot = fmaf(a, v.w - v.z, v.z);
+  return fmaf(b, bot - top, top);
+}
+
+// Column of a sample: clamped origin offset and weight
+template <int INTERP>
+__device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a) {
+  float xb;
+  if (INTERP == LCT_INTERP_TEX8)
+    xb = __fsub_rn(__fadd_rn(p_idx, 0.5f), 0.5f);
+  else
+    xb = p_idx;
+  const float fx = floorf(xb);
+  a = xb - fx;
+  if (INTERP == LCT_INTERP_TEX8) a = q8(a);
+  int i = (int)fx;
+  off = min(max(i, -2), ns) + 2;
+}
+
+template <int NZ, int INTERP, int MINB>
+__global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_constant__ BpQuadArgs A) {
+  __shared__ float s_c1[kQVB], s_s1[kQVB], s_c2[kQVB], s_s2[kQVB];
+  __shared__ int s_jlo[kQVB], s_jhi[kQVB];
+
+  const int tid = threadIdx.y * kQTX + threadIdx.x;
+  const int ix = blockIdx.x * kQTX + threadIdx.x;
+  const int iy = blockIdx.y * kQTY + threadIdx.y;
+  const int slab = blockIdx.z / A.zchunks;
+  const int z0 = (blockIdx.z % A.zchunks) * NZ;
+  const int nzc = min(NZ, A.nz - z0);
+
+  const float xc = ((float)ix - A.wx) * A.dx;
+  const float yc = ((float)iy - A.wy) * A.dy;
+  float zc[NZ];
+#pragma unroll
+  for (int j = 0; j < NZ; ++j) zc[j] = ((float)(z0 + j) - A.wz) * A.dz;
+
+  int vlo = INT_MAX, vhi = INT_MIN;
+  for (int j = 0; j < nzc; ++j) {
+    vlo = min(vlo, A.a_min[z0 + j]);
+    vhi = max(vhi, A.a_mid[z0 + j]);
+  }
+  const float4* quads = A.quads + (long long)A.slab_view[slab] * A.qstride;
+  const float* betas = A.betas + A.slab_view[slab];
+  const float wt = A.wt;
+
+  float acc[NZ];
+#pragma unroll
+  for (int j = 0; j < NZ; ++j) acc[j] = 0.0f;
+
+  for (int vb = vlo; vb < vhi; vb += kQVB) {
+    __syncthreads();
+    if (tid < kQVB && vb + tid < vhi) {
+      const int ia = vb + tid;
+      view_trig_pi(betas, ia, s_c1[tid], s_s1[tid]);
+      view_trig_pi(betas, ia + A.half, s_c2[tid], s_s2[tid]);
+      int jlo = nzc, jhi = 0;
+      for (int j = 0; j < nzc; ++j)
+        if (ia >= A.a_min[z0 + j] && ia < A.a_mid[z0 + j]) {
+          jlo = min(jlo, j);
+          jhi = max(jhi, j + 1);
+        }
+      s_jlo[tid] = jlo;
+      s_jhi[tid] = jhi;
+    }
+    __syncthreads();
+    const int nv = min(kQVB, vhi - vb);
+    for (int k = 0; k < nv; ++k) {
+      const int ia = vb + k;
+      const int jlo = s_jlo[k], jhi = s_jhi[k];
+      const float cb = s_c1[k], sb = s_s1[k], cb2 = s_c2[k], sb2 = s_s2[k];
+      // CUDA/Backprojector.cu:53-64, z-invariant part
+      const float phat = -xc * cb - yc * sb;
+      float theta, delta_p, tho, sq;
+      if (INTERP == LCT_INTERP_TEX8) {
+        theta = asinf(__fdiv_rn(phat, A.dso));
+        delta_p = __fdiv_rn(__fmul_rn(theta, A.dso), A.ds);
+        tho = __fdiv_rn(theta, A.orbit);
+        sq = sqrtf(fmaf(-phat, phat, A.dso2));
+      } else {
+        theta = asinf(phat * A.inv_dso);
+        delta_p = theta * A.dso_over_ds;
+        tho = theta * A.inv_orbit;
+        const float t = fmaf(-phat, phat, A.dso2);
+        sq = t * rsqrtf(t);
+      }
+      const float zr1 = fmaf((float)ia + tho, A.dzv, A.z0);
+      const float zr2 = fmaf((float)(ia + A.half) - tho, A.dzv, A.z0);
+      const float l1 = fmaf(xc, sb, fmaf(-yc, cb, sq));
+      const float l2 = fmaf(xc, sb2, fmaf(-yc, cb2, sq));
+      const float k1 = __fdividef(A.kq, l1), k2 = __fdividef(A.kq, l2);
+      const float m1 = -zr1 * k1, m2 = -zr2 * k2;
+      int o1, o2;
+      float a1, a2;
+      quad_col<INTERP>(delta_p + A.ws, A.ns, o1, a1);
+      quad_col<INTERP>(-delta_p + A.ws, A.ns, o2, a2);
+      const float4* q1 = quads + (long long)ia * A.qstride + o1;
+      const float4* q2 = quads + (long long)(ia + A.half) * A.qstride + o2;
+      auto slice = [&](int j) {
+        const float qh1 = fmaf(zc[j], k1, m1), qh2 = fmaf(zc[j], k2, m2);
+        const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
+        const float r = __fdividef(2.0f, qh1 - qh2);
+        float w1 = -qh2 * r, w2 = qh1 * r;
+        w1 = out1 ? (out2 ? 1.0f : 0.0f) : (out2 ? 2.0f : w1);
+        w2 = out1 ? (out2 ? 1.0f : 2.0f) : (out2 ? 0.0f : w2);
+        const float s1 = quad_sample<INTERP>(q1, A.qcols, A.nt, a1, qh1 + wt);
+        const float s2 = quad_sample<INTERP>(q2, A.qcols, A.nt, a2, qh2 + wt);
+        acc[j] = fmaf(w1, s1, fmaf(w2, s2, acc[j]));
+      };
+      if (jlo == 0 && jhi == NZ) {
+#pragma unroll
+        for (int j = 0; j < NZ; ++j) slice(j);
+      } else {
+#pragma unroll
+        for (int j = 0; j < NZ; ++j)
+          if (j >= jlo && j < jhi) slice(j);
+      }
+    }
+  }
+
+  if (ix < A.nx && iy < A.ny) {
+    float* out = A.img + ((long long)(A.slab_z0[slab] + z0) * A.ny + iy) * A.nx + ix;
+    const long long plane = (long long)A.nx * A.ny;
+#pragma unroll
+    for (int j = 0; j < NZ; ++j) {
+      if (j < nzc) {
+        const int span = A.a_max[z0 + j] - A.a_min[z0 + j];
+        // CUDA/Backprojector.cu:96, evaluated in double (PI is a double literal there)
+        out[j * plane] = span > 0 ? (float)((double)(acc[j] * 2.0f) * kRefPi / (double)(float)span) : 0.0f;
+      }
+    }
+  }
+}
+
+bool bp_windows_full(const lct_geom& g, const lct_img& ig, int nz) {
+  const float dzv = g.pitch / (float)g.n_proj_turn;
+  const int half = g.n_proj_turn / 2;
+  for (int z = 0; z < nz; ++z) {
+    BpWindow w = bp_window(g, ig, z, dzv, half);
+    if (!(w.a_min == w.a_mid - half && w.a_max == w.a_mid + half)) return false;
+  }
+  return true;
+}
+
+int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                        const float4* quads, cudaStream_t s) {
+  if (L.nz <= 0 || L.nz > kBpMaxZ || L.n_slabs <= 0 || L.n_slabs > kBpMaxSlabs) return LCT_ERR_ARG;
+  if (!bp_windows_full(g, ig, L.nz)) return LCT_ERR_UNSUPPORTED;
+  static thread_local BpQuadArgs a;
+  a.quads = quads;
+  a.betas = L.betas;
+  a.img = L.img;
+  a.qstride = quad_view_elems(g.ns, g.nt);
+  a.qcols = (int)quad_cols(g.ns);
+  a.ns = g.ns;
+  a.nt = g.nt;
+  a.n_angle = L.n_angle;
+  a.nx = ig.nx;
+  a.ny = ig.ny;
+  a.nz = L.nz;
+  a.ws = g.ws;
+  a.wt = g.wt;
+  a.ds = g.ds;
+  a.dso = g.dso;
+  a.dso2 = g.dso * g.dso;
+  a.inv_dso = 1.0f / g.dso;
+  a.dso_over_ds = g.dso / g.ds;
+  a.orbit = g.orbit;
+  a.inv_orbit = 1.0f / g.orbit;
+  a.z0 = g.source_z0;
+  a.dzv = g.pitch / (float)g.n_proj_turn;  // CUDA/Backprojector.cu:149
+  a.kq = g.dso * (float)g.z_dir / g.dt;
+  a.wx = ig.wx;
+  a.wy = ig.wy;
+  a.wz = ig.wz;
+  a.dx = ig.dx;
+  a.dy = ig.dy;
+  a.dz = ig.dz;
+  a.half = g.n_proj_turn / 2;  // CUDA/Backprojector.cu:148
+  for (int z = 0; z < L.nz; ++z) {
+    BpWindow w = bp_window(g, ig, z, a.dzv, a.half);
+    a.a_min[z] = w.a_min;
+    a.a_mid[z] = w.a_mid;
+    a.a_max[z] = w.a_max;
+  }
+  for (int i = 0; i < L.n_slabs; ++i) {
+    a.slab_view[i] = L.slab_view[i];
+    a.slab_z0[i] = L.slab_z0[i];
+  }
+  int nzt = L.nz_thread;
+  if (nzt != 4 && nzt != 8 && nzt != 16) nzt = 8;
+  a.zchunks = (L.nz + nzt - 1) / nzt;
+  dim3 grid((ig.nx + kQTX - 1) / kQTX, (ig.ny + kQTY - 1) / kQTY, L.n_slabs * a.zchunks);
+  if (grid.z > 65535) return LCT_ERR_ARG;
+  dim3 block(kQTX, kQTY);
+  const bool tex = L.interp == LCT_INTERP_TEX8;
+  int minb = L.minb;
+  if (minb < 1 || minb > 4) minb = 4;  // measured best on B200 (4 CTAs x 256 threads per SM)
+#define LCT_BPQ(NZV, MB)                                                                  \
+  do {                                                                                    \
+    if (tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB><<<grid, block, 0, s>>>(a);          \
+    else bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB><<<grid, block, 0, s>>>(a);             \
+  } while (0)
+#define LCT_BPQ_NZ(NZV)            \
+  do {                             \
+    switch (minb) {                \
+      case 1: LCT_BPQ(NZV, 1); break; \
+      case 3: LCT_BPQ(NZV, 3); break; \
+      case 4: LCT_BPQ(NZV, 4); break; \
+      default: LCT_BPQ(NZV, 2);    \
+    }                              \
+  } while (0)
+  switch (nzt) {
+    case 4: LCT_BPQ_NZ(4); break;
+    case 16: LCT_BPQ_NZ(16); break;
+    default: LCT_BPQ_NZ(8);
+  }
+#undef LCT_BPQ_NZ
+#undef LCT_BPQ
+  return launch_status();
+}
+
+}  // namespace lct

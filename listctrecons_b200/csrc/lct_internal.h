@@ -8,6 +8,11 @@
 #include "lct.h"
 
 #define LCT_API extern "C" __attribute__((visibility("default")))
+#ifdef __CUDACC__
+#define LCT_HD __host__ __device__
+#else
+#define LCT_HD
+#endif
 
 namespace lct {
 
@@ -57,8 +62,24 @@ struct BpLaunch {
   int slab_z0[kBpMaxSlabs];
   int interp, addr;
   int nz_thread;       // slices per thread (8, 16, 32; 0 = choose)
+  int minb = 0;        // quad kernel: resident CTAs per SM the register budget targets (0 = 4)
 };
 int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaStream_t s);
+
+// Filtered views in quad layout for the backprojector.  Per view, entry (j, i) for
+// j in [-2, nt], i in [-2, ns] (stored at (j + 2) * (ns + 3) + (i + 2)) holds the 2 x 2 texel
+// block {T(j, i), T(j, i+1), T(j+1, i), T(j+1, i+1)}, texels outside the detector read as 0
+// (LCT_ADDR_BORDER) or clamped to the edge (LCT_ADDR_CLAMP).  A bilinear sample is then one
+// 16-byte load at its clamped origin; the padding ring makes every clamped origin valid.
+LCT_HD inline long long quad_cols(int ns) { return (long long)ns + 3; }
+LCT_HD inline long long quad_view_elems(int ns, int nt) { return (long long)(nt + 3) * (ns + 3); }
+int launch_quad_pack(const float* rows, long long views, int ns, int nt, int addr, float4* quads,
+                     cudaStream_t s);
+// Backprojection from quad-layout views (full windows only; L.proj is ignored, L.quads used).
+int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                        const float4* quads, cudaStream_t s);
+// True when every slice window of the block is a full rotation (the pairs kernels apply).
+bool bp_windows_full(const lct_geom& g, const lct_img& ig, int nz);
 
 // Rebinning, scan mode: each global parallel view g in [g0, g0 + nviews) is interpolated
 // from the fan buffer whose view 0 is global fan view `fan_first`, with the view shift of

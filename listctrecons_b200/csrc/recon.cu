@@ -35,6 +35,8 @@ struct lct_recon {
   float* d_betas = nullptr;
   float* d_h = nullptr;
   float* d_img = nullptr;
+  float4* d_quad = nullptr;  // filtered views in quad layout (backprojection input)
+  bool quads = false;        // full windows: the quad-layout pairs kernel applies
   cudaEvent_t ev[6] = {};
   float times[5] = {};
   int device = 0;
@@ -51,16 +53,18 @@ static void free_recon(lct_recon* r) {
   cudaFree(r->d_betas);
   cudaFree(r->d_h);
   cudaFree(r->d_img);
+  cudaFree(r->d_quad);
   for (auto& e : r->ev)
     if (e) cudaEventDestroy(e);
   delete r;
 }
 
 static int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
-  if (requested == 8 || requested == 16 || requested == 32) return requested;
-  // slices a view stays active for: (feed/2) / dz
+  if (requested == 4 || requested == 8 || requested == 16) return requested;
+  // slices a view stays active for: (feed/2) / dz; measured best: 8 unless views are active
+  // for only a few slices
   const double act = 0.5 * (double)g.pitch / (double)ig.dz;
-  return act >= 20.0 ? 16 : 8;
+  return act < 6.0 ? 4 : 8;
 }
 
 // kernels one filter call launches
@@ -87,6 +91,7 @@ LCT_API void lct_recon_opts_default(lct_recon_opts* o) {
   o->interp = LCT_INTERP_TEX8;
   o->addr = LCT_ADDR_BORDER;
   o->bp_nz = 0;
+  o->bp_minb = 0;
 }
 
 LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out) {
@@ -159,6 +164,11 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
     if ((st = cuda_status(cudaMalloc(&r->d_betas, sizeof(float) * readings)))) break;
     if ((st = cuda_status(cudaMalloc(&r->d_h, sizeof(float) * 2 * g.ns)))) break;
     if ((st = cuda_status(cudaMalloc(&r->d_img, sizeof(float) * img_elems)))) break;
+    r->quads = o.backprojector == LCT_BP_PAR && bp_windows_full(g, r->info.ig, kBlockSlices);
+    if (r->quads &&
+        (st = cuda_status(cudaMalloc(&r->d_quad, sizeof(float4) * par_views *
+                                                     quad_view_elems(g.ns, g.nt)))))
+      break;
     if ((st = cuda_status(cudaMemcpy(r->d_betas, plan_angles(plan), sizeof(float) * readings,
                                      cudaMemcpyHostToDevice))))
       break;
@@ -279,7 +289,14 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
         L.interp = r->o.interp;
         L.addr = addr;
         L.nz_thread = bp_nz;
-        st = launch_bp_par(g, ig, L, s);
+        L.minb = r->o.bp_minb;
+        if (r->quads) {
+          if ((st = launch_quad_pack(r->d_par, g.n_angle, g.ns, g.nt, addr, r->d_quad, s))) return st;
+          r->launches++;
+          st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
+        } else {
+          st = launch_bp_par(g, ig, L, s);
+        }
       }
       if (st) return st;
       r->launches++;
@@ -311,6 +328,15 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, r->g_count * g.nt, r->o.filter_mode, s)))
       return st;
     r->launches += filter_launches(r->o.filter_mode);
+    if (r->quads && r->o.backprojector == LCT_BP_PAR) {
+      // border-addressed quads; a clamped (legacy first) slab reads the FP32 views directly
+      if ((st = launch_quad_pack(r->d_par, r->g_count, g.ns, g.nt, LCT_ADDR_CLAMP == r->o.addr
+                                                                      ? LCT_ADDR_CLAMP
+                                                                      : LCT_ADDR_BORDER,
+                                 r->d_quad, s)))
+        return st;
+      r->launches++;
+    }
     if ((st = cuda_status(cudaEventRecord(r->ev[3], s)))) return st;
     if (r->o.backprojector == LCT_BP_PI_ORI) {
       for (int b = 0; b < nb; ++b) {
@@ -343,9 +369,15 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
         L.interp = r->o.interp;
         L.addr = addr;
         L.nz_thread = bp_nz;
+        L.minb = r->o.bp_minb;
         // betas are indexed by the same slab offset: shift the base by g_first
         L.betas = r->d_betas + r->g_first;
-        if ((st = launch_bp_par(g, ig, L, s))) return st;
+        const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+        if (r->quads && addr == packed)
+          st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
+        else
+          st = launch_bp_par(g, ig, L, s);
+        if (st) return st;
         r->launches++;
         b0 = b1;
       }
