@@ -32,6 +32,7 @@ extern "C" {
 #define LCT_ERR_DEVICE 5      /* a kernel raised the device status word */
 #define LCT_ERR_UNSUPPORTED 6 /* option not available for this geometry / build */
 #define LCT_ERR_IO 7          /* file missing or short */
+#define LCT_ERR_SCRATCH 8     /* larger than the fixed scratch of an allocation-free entry point */
 
 typedef void* lct_stream; /* cudaStream_t; NULL = the legacy default stream */
 
@@ -140,6 +141,17 @@ int lct_filter_rows(int ns, const float* d_h, float* d_rows, int64_t nrows, int 
 int lct_backproject_par(const lct_geom* g, const lct_img* ig, const float* d_betas,
                         const float* d_proj, float* d_img, int interp, int addr,
                         lct_stream stream);
+/* No counterpart in the reference.  lct_backproject_par for callers that cannot let the
+   library allocate device memory (a host that budgets all device memory itself, an acquisition
+   loop that must not stall or fail on an allocation, a plugin host with its own allocator): the
+   quad-layout scratch comes from a fixed 64 MiB array in the library that every GPU loading it
+   holds until exit, and nothing is allocated.  Blocks needing more than 64 MiB of scratch
+   (n_angle*(nt+3)*(ns+3)*16 bytes) return LCT_ERR_SCRATCH before any launch.  All calls on a
+   device share that array: calls that overlap on the GPU race.  The first call on a device
+   resolves the array's address and should come before any stream capture. */
+int lct_backproject_par_noalloc(const lct_geom* g, const lct_img* ig, const float* d_betas,
+                                const float* d_proj, float* d_img, int interp, int addr,
+                                lct_stream stream);
 /* PiOriBackprojectorGPU::backproject + backprojection_cbct_pi_ori_kernel
    (CUDA/Backprojector.cu:171-307). */
 int lct_backproject_pi_ori(const lct_geom* g, const lct_img* ig, const float* d_betas,

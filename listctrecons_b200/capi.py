@@ -19,6 +19,7 @@ LCT_ERR_RANGE = 4
 LCT_ERR_DEVICE = 5
 LCT_ERR_UNSUPPORTED = 6
 LCT_ERR_IO = 7
+LCT_ERR_SCRATCH = 8
 
 INTERP_TEX8, INTERP_EXACT = 0, 1
 ADDR_BORDER, ADDR_CLAMP, ADDR_LEGACY = 0, 1, 2
@@ -135,6 +136,7 @@ SIGNATURES: dict[str, tuple] = {
     "lct_filter_taps": (I32, [I32, I32, I32, F32, P]),
     "lct_filter_rows": (I32, [I32, P, P, I64, I32, P]),
     "lct_backproject_par": (I32, [GP, IP, P, P, P, I32, I32, P]),
+    "lct_backproject_par_noalloc": (I32, [GP, IP, P, P, P, I32, I32, P]),
     "lct_backproject_pi_ori": (I32, [GP, IP, P, P, P, I32, I32, P]),
     "lct_plan_create": (I32, [C.POINTER(ScanParams), P, P, C.POINTER(P)]),
     "lct_plan_info_get": (I32, [P, C.POINTER(PlanInfo)]),

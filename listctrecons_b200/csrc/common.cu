@@ -80,6 +80,7 @@ LCT_API const char* lct_status_string(int status) {
     case LCT_ERR_DEVICE: return "device status word raised";
     case LCT_ERR_UNSUPPORTED: return "unsupported option";
     case LCT_ERR_IO: return "file missing or short";
+    case LCT_ERR_SCRATCH: return "problem larger than the fixed scratch of the allocation-free entry point";
     default: return "unknown status";
   }
 }
