@@ -379,7 +379,7 @@ def run_ours(args, rank, world, dist):
         "e2e": {"value": e2e, "unit": UNIT, "s_per_volume": e2e_ms / 1e3,
                 "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
         "gpu_launches": launches,
-        "roofline": {"kernel": "bp_par_pairs_kernel", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": "bp_quad_kernel", "bound": "hbm", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes": alg_bytes, "launch_ms": bp},
