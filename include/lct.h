@@ -126,6 +126,7 @@ int lct_filter_taps(int kind, int window, int ns, float ds, float* h);
 
 #define LCT_FILTER_FP32 0  /* FP32 FMA in the reference's summation order (bit-exact) */
 #define LCT_FILTER_BF16X3 1 /* Toeplitz GEMM on tcgen05, BF16 hi/lo split, FP32 accumulate */
+#define LCT_FILTER_BF16X6 2 /* the same with 3-way splits and 6 products (FP32-level error) */
 
 /* Filter::filter + filter_kernel (CUDA/Filter.cu:10-73): rows[r][is] <-
    sum_k h[is-k+ns] * rows[r][k] for r < nrows, in place (device pointers; d_h has 2*ns). */

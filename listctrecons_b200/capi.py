@@ -25,7 +25,7 @@ INTERP_TEX8, INTERP_EXACT = 0, 1
 ADDR_BORDER, ADDR_CLAMP, ADDR_LEGACY = 0, 1, 2
 FILTER_RAMLAK, FILTER_SHEPP_LOGAN = 0, 1
 WINDOW_NONE, WINDOW_HANN, WINDOW_HAMMING, WINDOW_COSINE = 0, 1, 2, 3
-FILTER_FP32, FILTER_BF16X3 = 0, 1
+FILTER_FP32, FILTER_BF16X3, FILTER_BF16X6 = 0, 1, 2
 MODE_BLOCK, MODE_SCAN = 0, 1
 REBIN_FAN2PAR, REBIN_NULL, REBIN_PI_ORI = 0, 1, 2
 PW_NONE, PW_PI_ORI = 0, 1

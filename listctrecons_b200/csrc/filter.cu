@@ -137,13 +137,12 @@ __global__ void __launch_bounds__(kFiltThreads) filter_fp32_kernel(const float* 
   }
 }
 
-int launch_filter_bf16x3(int ns, const float* d_h, float* d_rows, long long nrows,
-                         cudaStream_t s);  // filter_tc.cu
 
 int launch_filter_rows(int ns, const float* d_h, float* d_rows, long long nrows, int mode,
                        cudaStream_t s) {
   if (nrows <= 0) return LCT_OK;
-  if (mode == LCT_FILTER_BF16X3) return launch_filter_bf16x3(ns, d_h, d_rows, nrows, s);
+  if (mode == LCT_FILTER_BF16X3 || mode == LCT_FILTER_BF16X6)
+    return launch_filter_tc(ns, d_h, d_rows, nrows, mode, s);
   const int nsp = (ns + 3) / 4 * 4;
   const size_t smem = sizeof(float) * (filt_rows_offset(ns) + (size_t)kFiltRows * nsp);
   static bool attr_set[64] = {false};
@@ -167,6 +166,7 @@ int launch_filter_rows(int ns, const float* d_h, float* d_rows, long long nrows,
 LCT_API int lct_filter_rows(int ns, const float* d_h, float* d_rows, int64_t nrows, int mode,
                             lct_stream stream) {
   if (ns <= 0 || ns > 3072 || !d_h || !d_rows || nrows < 0) return LCT_ERR_ARG;
-  if (mode != LCT_FILTER_FP32 && mode != LCT_FILTER_BF16X3) return LCT_ERR_ARG;
+  if (mode != LCT_FILTER_FP32 && mode != LCT_FILTER_BF16X3 && mode != LCT_FILTER_BF16X6)
+    return LCT_ERR_ARG;
   return launch_filter_rows(ns, d_h, d_rows, nrows, mode, (cudaStream_t)stream);
 }

@@ -88,6 +88,15 @@ int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long f
                               long long fan_count, float* d_par, long long g0,
                               long long nviews, int interp, int addr, cudaStream_t s);
 
+// BF16x3 tensor-core filter with caller-owned scratch (filter_tc.cu): tc_scratch_bytes() for
+// rows_cap rows; tc_build_toeplitz once per taps, then tc_filter per batch of rows (in place).
+size_t tc_scratch_bytes(int ns, long long rows_cap, int mode);
+int tc_build_toeplitz(int ns, const float* d_h, void* scratch, int mode, cudaStream_t s);
+int tc_filter(int ns, float* d_rows, long long nrows, void* scratch, long long rows_cap, int mode,
+              cudaStream_t s);
+int launch_filter_tc(int ns, const float* d_h, float* d_rows, long long nrows, int mode,
+                     cudaStream_t s);
+
 // Filter over nrows rows of ns samples (filter.cu).
 int launch_filter_rows(int ns, const float* d_h, float* d_rows, long long nrows, int mode,
                        cudaStream_t s);

@@ -36,6 +36,8 @@ struct lct_recon {
   float* d_h = nullptr;
   float* d_img = nullptr;
   float4* d_quad = nullptr;  // filtered views in quad layout (backprojection input)
+  void* d_tc = nullptr;      // BF16x3 filter operands (row and Toeplitz planes)
+  long long tc_rows = 0;
   bool quads = false;        // full windows: the quad-layout pairs kernel applies
   cudaEvent_t ev[6] = {};
   float times[5] = {};
@@ -54,6 +56,7 @@ static void free_recon(lct_recon* r) {
   cudaFree(r->d_h);
   cudaFree(r->d_img);
   cudaFree(r->d_quad);
+  cudaFree(r->d_tc);
   for (auto& e : r->ev)
     if (e) cudaEventDestroy(e);
   delete r;
@@ -68,7 +71,7 @@ static int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
 }
 
 // kernels one filter call launches
-static int filter_launches(int mode) { return mode == LCT_FILTER_BF16X3 ? 2 : 1; }
+static int filter_launches(int mode) { return mode == LCT_FILTER_FP32 ? 1 : 2; }
 
 static int block_addr(const lct_recon* r, int b) {
   if (r->o.addr == LCT_ADDR_LEGACY) return b == 0 ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
@@ -108,7 +111,7 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
   if (o.backprojector != LCT_BP_PAR && o.backprojector != LCT_BP_PI_ORI) return LCT_ERR_ARG;
   if (o.interp != LCT_INTERP_TEX8 && o.interp != LCT_INTERP_EXACT) return LCT_ERR_ARG;
   if (o.addr < LCT_ADDR_BORDER || o.addr > LCT_ADDR_LEGACY) return LCT_ERR_ARG;
-  if (o.filter_mode != LCT_FILTER_FP32 && o.filter_mode != LCT_FILTER_BF16X3) return LCT_ERR_ARG;
+  if (o.filter_mode < LCT_FILTER_FP32 || o.filter_mode > LCT_FILTER_BF16X6) return LCT_ERR_ARG;
   if (o.mode == LCT_MODE_SCAN && o.rebinner == LCT_REBIN_PI_ORI) return LCT_ERR_UNSUPPORTED;
 
   lct_recon* r = new (std::nothrow) lct_recon;
@@ -177,6 +180,13 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
     if ((st = cuda_status(cudaMemcpy(r->d_h, h.data(), sizeof(float) * h.size(),
                                      cudaMemcpyHostToDevice))))
       break;
+    if (o.filter_mode != LCT_FILTER_FP32) {
+      r->tc_rows = par_views * g.nt;
+      if ((st = cuda_status(cudaMalloc(&r->d_tc, tc_scratch_bytes(g.ns, r->tc_rows, o.filter_mode)))))
+        break;
+      if ((st = tc_build_toeplitz(g.ns, r->d_h, r->d_tc, o.filter_mode, 0))) break;
+      if ((st = cuda_status(cudaDeviceSynchronize()))) break;
+    }
     for (auto& e : r->ev)
       if ((st = cuda_status(cudaEventCreate(&e)))) break;
   } while (0);
@@ -223,6 +233,12 @@ static int run_rebin(lct_recon* r, const lct_geom& g, const float* fan_block, fl
   }
 }
 
+static int run_filter(lct_recon* r, const lct_geom& g, long long nrows, cudaStream_t s) {
+  if (r->o.filter_mode != LCT_FILTER_FP32)
+    return tc_filter(g.ns, r->d_par, nrows, r->d_tc, r->tc_rows, r->o.filter_mode, s);
+  return launch_filter_rows(g.ns, r->d_h, r->d_par, nrows, LCT_FILTER_FP32, s);
+}
+
 LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                           float* image, int image_on_device, lct_stream stream) {
   if (!r || !fan || !image) return LCT_ERR_ARG;
@@ -267,9 +283,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
         if ((st = lct_weight_pi_ori(&g, r->d_par, s))) return st;
         r->launches++;
       }
-      if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, (long long)g.n_angle * g.nt,
-                                   r->o.filter_mode, s)))
-        return st;
+      if ((st = run_filter(r, g, (long long)g.n_angle * g.nt, s))) return st;
       r->launches += filter_launches(r->o.filter_mode);
       const float* betas = r->d_betas + bi.block_proj_start + g.add_projections;
       float* img_b = d_img + (long long)b * slab;
@@ -325,8 +339,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
       r->launches++;
     }
     if ((st = cuda_status(cudaEventRecord(r->ev[2], s)))) return st;
-    if ((st = launch_filter_rows(g.ns, r->d_h, r->d_par, r->g_count * g.nt, r->o.filter_mode, s)))
-      return st;
+    if ((st = run_filter(r, g, r->g_count * g.nt, s))) return st;
     r->launches += filter_launches(r->o.filter_mode);
     if (r->quads && r->o.backprojector == LCT_BP_PAR) {
       // border-addressed quads; a clamped (legacy first) slab reads the FP32 views directly
