@@ -66,7 +66,10 @@ __global__ void __launch_bounds__(256) quad_pack_kernel(const float* __restrict_
   };
   for (int q = threadIdx.x; q < ns + 3; q += blockDim.x) {
     const int i = q - 2;
-    out[q] = make_float4(texel(j, i), texel(j, i + 1), texel(j + 1, i), texel(j + 1, i + 1));
+    const float t00 = texel(j, i), t01 = texel(j, i + 1), t10 = texel(j + 1, i),
+                t11 = texel(j + 1, i + 1);
+    // differences: a bilinear sample is then T00 + a dx + b (dy + a dxy), three FMAs
+    out[q] = make_float4(t00, t01 - t00, t10 - t00, (t11 - t10) - (t01 - t00));
   }
 }
 
@@ -96,16 +99,15 @@ __device__ __forceinline__ float quad_sample(const float4* __restrict__ qb, int 
   float b = yb - fy;
   int j = (int)fy;
   j = min(max(j, -2), nt);
-  const float4 v = __ldg(qb + (j + 2) * qcols);
+  const float4 v = __ldg(qb + (j + 2) * qcols);  // T00, dx, dy, dxy
   if (INTERP == LCT_INTERP_TEX8) {
+    // texture unit: w01 = a - w11, w10 = b - w11, w00 = 1 - a - b + w11, so the sample is
+    // T00 + a dx + b dy + w11 dxy with w11 = round-half-up(a b) on the 1/256 grid
     b = q8(b);
-    float w00, w01, w10, w11;
-    tex_bilinear_weights(a, b, w00, w01, w10, w11);
-    return fmaf(w11, v.w, fmaf(w10, v.z, fmaf(w01, v.y, w00 * v.x)));
+    const float w11 = floorf(a * b * 256.0f + 0.5f) * (1.0f / 256.0f);
+    return fmaf(w11, v.w, fmaf(b, v.z, fmaf(a, v.y, v.x)));
   }
-  const float top = fmaf(a, v.y - v.x, v.x);
-  const float bot = fmaf(a, v.w - v.z, v.z);
-  return fmaf(b, bot - top, top);
+  return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
 }
 
 // Column of a sample: clamped origin offset and weight
