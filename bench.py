@@ -145,10 +145,11 @@ def make_workload(name: str, rank: int, world: int, blocks: int = 0):
     fov = 0.5 * min(geo.nx * geo.dx, geo.ny * geo.dx)
     ph = Phantom.random(w["ellipsoids"], seed=20240 + w["ellipsoids"], fov_radius=fov,
                         z_lo=lo, z_hi=hi)
-    geo.max_blocks = w["blocks"]
-    geo.first_block = rank * w["blocks"]
+    from listctrecons_b200.shard import shard_blocks
+
+    first, count = shard_blocks(full.info.n_blocks, world, rank, per_rank=w["blocks"])
     params = geo.scan_params()
-    params.first_block = geo.first_block
+    params.first_block, params.max_blocks = first, count
     plan = Plan(params=params, angles32=geo.angles32(), zpos32=geo.zpos32())
     return w, geo, plan, ph
 
@@ -177,6 +178,44 @@ def oracle_accuracy(w, geo, plan, fan_block_views, img, interp, rows=2):
         out["fp64_exact"] = out["same_formulas"]
     out["sample"] = f"block {plan.info.first_block}, rows y={y0}..{y0 + rows - 1}, all x, 32 slices"
     return out
+
+
+def plain_gpu(w, geo, ph, ours_value):
+    """The reference program built from its own sources (oracle/_ref/ref_timed) on the same scan:
+    its per-block flow (pageable copies, per-block rebin/filter/BP with texture references).
+    It has no z-range key, so it reconstructs every block the scan allows; its reconstruct()
+    time is scaled to this workload's block count (blocks are equal work)."""
+    import torch
+
+    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.scan import simulate_gpu, write_scan_files
+
+    ref = ROOT / "oracle" / "_ref" / "ref_timed"
+    if not ref.exists():
+        return {"unavailable": "oracle/_ref/ref_timed not built"}
+    g2 = type(geo)(**{k: getattr(geo, k) for k in geo.__dataclass_fields__})
+    g2.max_blocks = 0
+    nb_all = Plan(g2).info.n_blocks
+    fan = simulate_gpu(g2, ph, i0=1e5, seed=7).cpu().numpy()
+    torch.cuda.empty_cache()
+    with tempfile.TemporaryDirectory() as td:
+        prm = write_scan_files(g2, fan, Path(td) / "data", Path(td) / "out")
+        del fan
+        r = subprocess.run([str(ref), str(prm)], capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        return {"unavailable": "reference program failed: " + r.stdout[-300:]}
+    rec = json.loads(r.stdout.strip().splitlines()[-1])
+    secs = rec["reconstruct_seconds"] * w["blocks"] / rec["n_blocks"]
+    plan = Plan(g2)
+    from listctrecons_b200.recon import Reconstruction
+
+    upd = Reconstruction(plan).stats().voxel_updates * w["blocks"] / nb_all
+    v = upd / secs / 1e9
+    return {"value": v, "unit": UNIT, "s_per_volume": secs, "blocks_timed": rec["n_blocks"],
+            "speedup_e2e": ours_value / v,
+            "what": "reference program (all Src/*.cpp + CUDA/*.cu built from its sources, legacy "
+                    "texture references via a compat header) reconstruct() time incl. its per-block "
+                    "file reads, scaled from its blocks to this workload's"}
 
 
 def cpu_port_sample(w, geo, plan, fan_block_views, budget_s: float):
@@ -400,6 +439,9 @@ def run_ours(args, rank, world, dist):
         fb = fan[lo: lo + g.n_angle_add].cpu().numpy()
         line["cpu_baseline"] = {k: v for k, v in cpu_port_sample(w, geo, plan, fb, args.cpu_budget).items()
                                 if k != "s_per_volume"}
+    if args.plain_gpu and world == 1:
+        del fan, h_fan
+        line["plain_gpu"] = plain_gpu(w, geo, ph, line["e2e"]["value"])
     print(json.dumps(line), flush=True)
     return 0
 
@@ -424,6 +466,8 @@ def main() -> int:
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plain-gpu", action="store_true",
+                    help="also time the reference program itself on the same scan (slow)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
