@@ -154,6 +154,116 @@ def make_workload(name: str, rank: int, world: int, blocks: int = 0):
     return w, geo, plan, ph
 
 
+CFG3_LABEL = ("batched helical FDK: 24 seeded scans, rows {16,32,64}, 672-896 cols, pitch "
+              "U[0.5,1.5], 2-20 rot, 256^2x32..512^2x128, one graph launch per stage")
+
+
+def make_cfg3(seed: int, n: int = 24):
+    """The batched configuration: uneven seeded scans (rotations raised to the planner minimum
+    where the drawn length plans too few blocks, MaxBlocks caps the volume)."""
+    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.scan import Phantom, ScanGeometry
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        nt = int(rng.choice([16, 32, 64]))
+        ns = int(rng.choice([672, 736, 800, 896]))
+        ds = float(rng.choice([0.5, 0.6])) if ns >= 800 else 0.6
+        npt = int(rng.choice([1000, 1152, 1200]))
+        pitch = float(rng.uniform(0.5, 1.5))
+        rot = float(rng.uniform(2, 20))
+        nx = int(rng.choice([256, 384, 512]))
+        blocks = int(rng.choice([1, 2, 4]))
+        dz = float(rng.choice([0.5, 0.75, 1.0]))
+        geo = ScanGeometry(ns=ns, nt=nt, ds=ds, dt=ds, npt=npt, pitch=pitch, nx=nx, ny=nx,
+                           dx=0.5 * 512 / nx, dz=dz)
+        need = geo.with_blocks(blocks)
+        geo.readings = max(int(round(rot * npt)), need.readings)
+        geo.max_blocks = blocks
+        p = Plan(geo)
+        lo = min(p.blocks[0].block_start, p.blocks[blocks - 1].block_end)
+        hi = max(p.blocks[0].block_start, p.blocks[blocks - 1].block_end)
+        ph = Phantom.random(10, seed=seed * 100 + i, fov_radius=0.5 * nx * geo.dx, z_lo=lo,
+                            z_hi=hi, semi=(5.0, 60.0))
+        out.append((geo, p, ph))
+    return out
+
+
+def run_batch(args, rank, world, dist):
+    """Config 3 through lct_batch (weak scaling: each rank its own 24-scan batch)."""
+    import torch
+
+    from listctrecons_b200 import capi
+    from listctrecons_b200.recon import Batch
+    from listctrecons_b200.scan import simulate_gpu
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    scans = make_cfg3(1000 + rank)
+    interp = capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT
+    fmode = {"fp32": capi.FILTER_FP32, "bf16x3": capi.FILTER_BF16X3, "bf16x6": capi.FILTER_BF16X6}[args.filter]
+    b = Batch([p for _, p, _ in scans], interp=interp, filter_mode=fmode, bp_nz=args.bp_nz,
+              bp_minb=args.bp_minb)
+    fans, v0 = [], []
+    for (geo, p, ph), (f0, fc) in zip(scans, b.fan_ranges):
+        fans.append(simulate_gpu(geo, ph, i0=1e5, seed=7, v0=f0, v1=f0 + fc))
+        v0.append(f0)
+    imgs = [torch.empty(sh, dtype=torch.float32, device=dev) for sh in b.image_shapes]
+    st = b.stats()
+    for _ in range(args.warmup):
+        b.run(fans, imgs, fan_view0=v0)
+    torch.cuda.synchronize()
+
+    def maxr(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    if dist is not None:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.run(fans, imgs, fan_view0=v0)
+        stage.append(b.last_times())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = maxr(e0.elapsed_time(e1) / args.steps)
+    hf = [f.cpu().pin_memory() for f in fans]
+    hi = [torch.empty(sh, dtype=torch.float32).pin_memory() for sh in b.image_shapes]
+    b.run(hf, hi, fan_view0=v0)
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        b.run(hf, hi, fan_view0=v0)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = maxr(e2.elapsed_time(e3) / args.steps)
+    if rank != 0:
+        return 0
+    upd = st.voxel_updates * world
+    line = {
+        "metric": METRIC, "value": upd / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (24 seeded 10-ellipsoid phantoms, helical scans simulated on the GPU)",
+        "config": {"workload": CFG3_LABEL, "scans": len(scans), "interp": args.interp,
+                   "filter": args.filter,
+                   "voxels": int(sum(np.prod(sh) for sh in b.image_shapes))},
+        "stages_ms": {k: statistics.mean(t[k] for t in stage) for k in stage[0]},
+        "e2e": {"value": upd / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "s_per_batch": e2e_ms / 1e3,
+                "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
+        "gpu_launches_note": "per step: 3 graph launches (rebin, filter, one persistent BP)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def oracle_accuracy(w, geo, plan, fan_block_views, img, interp, rows=2):
     """rel-L2 / max-abs of slab 0 rows against the FP64 oracle of the same formulas (texture
     emulation for TEX8) and against the unquantised FP64 oracle."""
@@ -452,7 +562,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3"])
     ap.add_argument("--mode", default="scan", choices=["scan", "block"])
     ap.add_argument("--filter", default="bf16x6", choices=["fp32", "bf16x3", "bf16x6"],
                     help="bf16x6: tensor-core Toeplitz GEMM with 3-way bf16 splits (meets the "
@@ -490,6 +600,8 @@ def main() -> int:
     else:
         torch.cuda.set_device(0)
     try:
+        if args.workload == "cfg3":
+            return run_batch(args, rank, world, dist)
         return run_ours(args, rank, world, dist)
     finally:
         if dist is not None:

@@ -237,8 +237,9 @@ typedef struct lct_recon_opts {
   int backprojector; /* LCT_BP_* */
   int interp;        /* LCT_INTERP_* */
   int addr;          /* LCT_ADDR_* */
-  int bp_nz;         /* backprojection slices per thread: 4, 8, 16 (0 = tuned) */
-  int bp_minb;       /* backprojection CTAs per SM the register budget targets: 1-4 (0 = tuned) */
+  int bp_nz;         /* backprojection slices per thread: 4, 8, 16; 0 = default (8, or 4 when a
+                        view stays active for few slices); -1 = autotune at create */
+  int bp_minb;       /* backprojection CTAs per SM the register budget targets: 1-4 (0 = 4) */
 } lct_recon_opts;
 
 void lct_recon_opts_default(lct_recon_opts* o);
@@ -253,6 +254,10 @@ int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon
    image: [n_blocks_run*32][ny][nx].  Returns after the image is complete (synchronous). */
 int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                   float* image, int image_on_device, lct_stream stream);
+/* Backprojection autotuner (no reference counterpart): times the kernel's slices-per-thread x
+   CTAs-per-SM variants on this recon's buffers, keeps the fastest in the recon, and caches it per
+   geometry class for the process.  Synchronous; returns the choice. */
+int lct_recon_autotune(lct_recon* r, int* nz, int* minb);
 /* Device-side per-stage time of the last run (ms): h2d, rebin, filter, backproject, d2h. */
 int lct_recon_last_times(const lct_recon* r, float* ms5);
 /* Fan views [first, first+count) the run reads (h2d bytes = count*nt*ns*4). */
@@ -268,6 +273,27 @@ typedef struct lct_recon_stats {
 } lct_recon_stats;
 int lct_recon_stats_get(const lct_recon* r, lct_recon_stats* out);
 void lct_recon_destroy(lct_recon* r);
+
+/* ---------------------------------------------------------------------------------------
+ * Batched reconstruction of many independent scans (no reference counterpart): one CUDA-graph
+ * launch per stage -- rebin, filter (+ quad pack), backprojection -- and the backprojection of
+ * every scan in ONE persistent work-list kernel over (scan, slab, tile) items.  Each scan's
+ * volume is bit-identical to its own lct_recon run with the same options.  Scan mode only.
+ * ------------------------------------------------------------------------------------- */
+typedef struct lct_batch lct_batch;
+int lct_batch_create(const lct_plan* const* plans, int n_scans, const lct_recon_opts* opts,
+                     lct_batch** out);
+/* fans[i]: scan i's views from fan_view0[i] on (host or device, as fan_on_device says);
+   images[i]: [n_blocks_run_i*32][ny][nx].  Synchronous. */
+int lct_batch_run(lct_batch* b, const float* const* fans, const int64_t* fan_view0,
+                  int fan_on_device, float* const* images, int image_on_device, lct_stream stream);
+/* Per-scan fan range and totals over the batch (voxel_updates, bytes, launches = graph and
+   copy launches of the last run). */
+int lct_batch_fan_range(const lct_batch* b, int scan, int64_t* first, int64_t* count);
+int lct_batch_stats_get(const lct_batch* b, lct_recon_stats* total);
+/* ms of the last run: upload, rebin graph, filter graph, backprojection graph, download */
+int lct_batch_last_times(const lct_batch* b, float* ms5);
+void lct_batch_destroy(lct_batch* b);
 
 /* ---------------------------------------------------------------------------------------
  * Scan simulator (no reference counterpart): analytic helical fan-beam line integrals of

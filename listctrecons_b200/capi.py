@@ -149,6 +149,13 @@ SIGNATURES: dict[str, tuple] = {
     "lct_recon_fan_range": (I32, [P, C.POINTER(I64), C.POINTER(I64)]),
     "lct_recon_stats_get": (I32, [P, C.POINTER(ReconStats)]),
     "lct_recon_destroy": (None, [P]),
+    "lct_recon_autotune": (I32, [P, C.POINTER(I32), C.POINTER(I32)]),
+    "lct_batch_create": (I32, [P, I32, C.POINTER(ReconOpts), C.POINTER(P)]),
+    "lct_batch_run": (I32, [P, P, P, I32, P, I32, P]),
+    "lct_batch_fan_range": (I32, [P, I32, C.POINTER(I64), C.POINTER(I64)]),
+    "lct_batch_stats_get": (I32, [P, C.POINTER(ReconStats)]),
+    "lct_batch_last_times": (I32, [P, P]),
+    "lct_batch_destroy": (None, [P]),
     "lct_sim_project": (I32, [P, I32, I32, I32, F32, F32, F32, F32, F32, P, P, I64, I64, F64, U64, P, P]),
     "lct_diag_tex3d_sample": (I32, [P, I32, I32, I32, P, I64, I32, P]),
 }

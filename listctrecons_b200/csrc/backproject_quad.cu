@@ -42,6 +42,7 @@ struct BpQuadArgs {
   float wx, wy, wz, dx, dy, dz;
   int half;
   int zchunks;
+  int gx, gy, gz;  // tile grid (work-list decoding)
   int slab_view[kBpMaxSlabs];
   int slab_z0[kBpMaxSlabs];
   int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
@@ -125,16 +126,18 @@ __device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a
   off = min(max(i, -2), ns) + 2;
 }
 
-template <int NZ, int INTERP, int MINB>
-__global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_constant__ BpQuadArgs A) {
+// One tile: voxel columns [bx*32, +32) x [by*8, +8), slab/slice chunk bz.  Called with
+// CTA-uniform arguments by every thread of a 256-thread CTA.
+template <int NZ, int INTERP>
+__device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by, int bz) {
   __shared__ float s_c1[kQVB], s_s1[kQVB], s_c2[kQVB], s_s2[kQVB];
   __shared__ int s_jlo[kQVB], s_jhi[kQVB];
 
   const int tid = threadIdx.y * kQTX + threadIdx.x;
-  const int ix = blockIdx.x * kQTX + threadIdx.x;
-  const int iy = blockIdx.y * kQTY + threadIdx.y;
-  const int slab = blockIdx.z / A.zchunks;
-  const int z0 = (blockIdx.z % A.zchunks) * NZ;
+  const int ix = bx * kQTX + threadIdx.x;
+  const int iy = by * kQTY + threadIdx.y;
+  const int slab = bz / A.zchunks;
+  const int z0 = (bz % A.zchunks) * NZ;
   const int nzc = min(NZ, A.nz - z0);
 
   const float xc = ((float)ix - A.wx) * A.dx;
@@ -240,6 +243,47 @@ __global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_
   }
 }
 
+template <int NZ, int INTERP, int MINB>
+__global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_constant__ BpQuadArgs A) {
+  bp_quad_tile<NZ, INTERP>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Persistent work list over several scans: item i belongs to the scan s with
+// prefix[s] <= i < prefix[s + 1] and is tile i - prefix[s] of that scan's grid.  Each CTA takes
+// items from *counter (zero before the launch) until the list is exhausted; a scan's tiles run
+// exactly the arithmetic of its own launch.
+template <int NZ, int INTERP, int MINB>
+__global__ void __launch_bounds__(kQTX* kQTY, MINB)
+    bp_quad_worklist_kernel(const BpQuadArgs* __restrict__ args, const int* __restrict__ prefix,
+                            int n_scans, int* __restrict__ counter) {
+  __shared__ BpQuadArgs sA;
+  __shared__ int s_item, s_scan;
+  const int tid = threadIdx.y * kQTX + threadIdx.x;
+  const int total = prefix[n_scans];
+  for (;;) {
+    __syncthreads();  // the previous tile is done with sA
+    if (tid == 0) {
+      const int item = atomicAdd(counter, 1);
+      int sc = 0;
+      while (sc + 1 < n_scans && prefix[sc + 1] <= item) ++sc;
+      s_item = item;
+      s_scan = sc;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= total) return;
+    const int* src = reinterpret_cast<const int*>(args + s_scan);
+    int* dst = reinterpret_cast<int*>(&sA);
+    for (int i = tid; i < (int)(sizeof(BpQuadArgs) / sizeof(int)); i += kQTX * kQTY) dst[i] = src[i];
+    __syncthreads();
+    const int local = item - prefix[s_scan];
+    const int bx = local % sA.gx;
+    const int by = (local / sA.gx) % sA.gy;
+    const int bz = local / (sA.gx * sA.gy);
+    bp_quad_tile<NZ, INTERP>(sA, bx, by, bz);
+  }
+}
+
 bool bp_windows_full(const lct_geom& g, const lct_img& ig, int nz) {
   const float dzv = g.pitch / (float)g.n_proj_turn;
   const int half = g.n_proj_turn / 2;
@@ -250,11 +294,10 @@ bool bp_windows_full(const lct_geom& g, const lct_img& ig, int nz) {
   return true;
 }
 
-int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
-                        const float4* quads, cudaStream_t s) {
+static int build_bp_quad_args(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                              const float4* quads, BpQuadArgs& a, int& nzt) {
   if (L.nz <= 0 || L.nz > kBpMaxZ || L.n_slabs <= 0 || L.n_slabs > kBpMaxSlabs) return LCT_ERR_ARG;
   if (!bp_windows_full(g, ig, L.nz)) return LCT_ERR_UNSUPPORTED;
-  static thread_local BpQuadArgs a;
   a.quads = quads;
   a.betas = L.betas;
   a.img = L.img;
@@ -295,11 +338,23 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
     a.slab_view[i] = L.slab_view[i];
     a.slab_z0[i] = L.slab_z0[i];
   }
-  int nzt = L.nz_thread;
+  nzt = L.nz_thread;
   if (nzt != 4 && nzt != 8 && nzt != 16) nzt = 8;
   a.zchunks = (L.nz + nzt - 1) / nzt;
-  dim3 grid((ig.nx + kQTX - 1) / kQTX, (ig.ny + kQTY - 1) / kQTY, L.n_slabs * a.zchunks);
-  if (grid.z > 65535) return LCT_ERR_ARG;
+  a.gx = (ig.nx + kQTX - 1) / kQTX;
+  a.gy = (ig.ny + kQTY - 1) / kQTY;
+  a.gz = L.n_slabs * a.zchunks;
+  if (a.gz > 65535) return LCT_ERR_ARG;
+  return LCT_OK;
+}
+
+int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                        const float4* quads, cudaStream_t s) {
+  static thread_local BpQuadArgs a;
+  int nzt = 8;
+  int st = build_bp_quad_args(g, ig, L, quads, a, nzt);
+  if (st) return st;
+  dim3 grid(a.gx, a.gy, a.gz);
   dim3 block(kQTX, kQTY);
   const bool tex = L.interp == LCT_INTERP_TEX8;
   int minb = L.minb;
@@ -325,6 +380,52 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
   }
 #undef LCT_BPQ_NZ
 #undef LCT_BPQ
+  return launch_status();
+}
+
+int bp_quad_args_size() { return (int)sizeof(BpQuadArgs); }
+
+int bp_quad_args_build(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                       const float4* quads, void* out, int* tiles) {
+  BpQuadArgs* a = static_cast<BpQuadArgs*>(out);
+  int nzt = 8;
+  int st = build_bp_quad_args(g, ig, L, quads, *a, nzt);
+  if (st) return st;
+  *tiles = a->gx * a->gy * a->gz;
+  return LCT_OK;
+}
+
+int launch_bp_quad_worklist(const void* d_args, const int* d_prefix, int n_scans, int* d_counter,
+                            int nz_thread, int interp, int minb, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (minb < 1 || minb > 4) minb = 4;
+  const BpQuadArgs* args = static_cast<const BpQuadArgs*>(d_args);
+  dim3 grid(sms * minb), block(kQTX, kQTY);
+  const bool tex = interp == LCT_INTERP_TEX8;
+#define LCT_BPW(NZV, MB)                                                                        \
+  do {                                                                                          \
+    if (tex)                                                                                    \
+      bp_quad_worklist_kernel<NZV, LCT_INTERP_TEX8, MB><<<grid, block, 0, s>>>(args, d_prefix, n_scans, d_counter); \
+    else                                                                                        \
+      bp_quad_worklist_kernel<NZV, LCT_INTERP_EXACT, MB><<<grid, block, 0, s>>>(args, d_prefix, n_scans, d_counter); \
+  } while (0)
+#define LCT_BPW_NZ(NZV)                  \
+  do {                                   \
+    switch (minb) {                      \
+      case 2: LCT_BPW(NZV, 2); break;    \
+      case 3: LCT_BPW(NZV, 3); break;    \
+      default: LCT_BPW(NZV, 4);          \
+    }                                    \
+  } while (0)
+  switch (nz_thread) {
+    case 4: LCT_BPW_NZ(4); break;
+    case 16: LCT_BPW_NZ(16); break;
+    default: LCT_BPW_NZ(8);
+  }
+#undef LCT_BPW_NZ
+#undef LCT_BPW
   return launch_status();
 }
 

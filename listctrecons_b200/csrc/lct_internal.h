@@ -81,6 +81,14 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
                         const float4* quads, cudaStream_t s);
 // True when every slice window of the block is a full rotation (the pairs kernels apply).
 bool bp_windows_full(const lct_geom& g, const lct_img& ig, int nz);
+// Work-list backprojection over several scans (batch): per-scan kernel arguments are built on
+// the host into an opaque record of bp_quad_args_size() bytes, copied to the device, and one
+// persistent launch runs every scan's tiles.
+int bp_quad_args_size();
+int bp_quad_args_build(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                       const float4* quads, void* out, int* tiles);
+int launch_bp_quad_worklist(const void* d_args, const int* d_prefix, int n_scans, int* d_counter,
+                            int nz_thread, int interp, int minb, cudaStream_t s);
 
 // Rebinning, scan mode: each global parallel view g in [g0, g0 + nviews) is interpolated
 // from the fan buffer whose view 0 is global fan view `fan_first`, with the view shift of

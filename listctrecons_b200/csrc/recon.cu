@@ -13,6 +13,8 @@
 //   img   n_blocks_run * 32 slices, block b at slice 32 b (CUDA/Backprojector.cu:158)
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -23,28 +25,7 @@ const float* plan_angles(const lct_plan* p);
 const lct_scan_params& plan_params(const lct_plan* p);
 }  // namespace lct
 
-struct lct_recon {
-  lct_plan_info info;
-  std::vector<lct_block_info> blocks;
-  lct_recon_opts o;
-  long long plane = 0;           // nt * ns
-  long long fan_first = 0, fan_count = 0;
-  long long g_first = 0, g_count = 0;  // scan mode
-  float* d_fan = nullptr;
-  float* d_par = nullptr;
-  float* d_betas = nullptr;
-  float* d_h = nullptr;
-  float* d_img = nullptr;
-  float4* d_quad = nullptr;  // filtered views in quad layout (backprojection input)
-  void* d_tc = nullptr;      // BF16x3 filter operands (row and Toeplitz planes)
-  long long tc_rows = 0;
-  bool quads = false;        // full windows: the quad-layout pairs kernel applies
-  cudaEvent_t ev[6] = {};
-  float times[5] = {};
-  int device = 0;
-  long long voxel_updates = 0;
-  int launches = 0;
-};
+#include "recon_internal.h"
 
 namespace lct {
 
@@ -63,7 +44,7 @@ static void free_recon(lct_recon* r) {
 }
 
 static int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
-  if (requested == 4 || requested == 8 || requested == 16) return requested;
+  if (requested == 4 || requested == 8 || requested == 16) return requested;  // else default
   // slices a view stays active for: (feed/2) / dz; measured best: 8 unless views are active
   // for only a few slices
   const double act = 0.5 * (double)g.pitch / (double)ig.dz;
@@ -194,7 +175,86 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
     free_recon(r);
     return st == LCT_ERR_CUDA && lct_last_cuda_error() == cudaErrorMemoryAllocation ? LCT_ERR_ALLOC : st;
   }
+  if (o.bp_nz == -1 && (st = lct_recon_autotune(r, nullptr, nullptr))) {
+    free_recon(r);
+    return st;
+  }
   *out = r;
+  return LCT_OK;
+}
+
+namespace lct {
+int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s);
+}
+
+// Backprojection autotuner: times the quad kernel over slices per thread x CTAs per SM on this
+// recon's own buffers and keeps the fastest; results are cached per geometry class (detector,
+// volume, window, interpolation and views-per-slice), so a class is tuned once per process.
+LCT_API int lct_recon_autotune(lct_recon* r, int* nz_out, int* minb_out) {
+  if (!r) return LCT_ERR_ARG;
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  if (r->o.mode != LCT_MODE_SCAN || !r->quads || r->o.addr == LCT_ADDR_LEGACY) {
+    if (nz_out) *nz_out = pick_bp_nz(g, ig, r->o.bp_nz);
+    if (minb_out) *minb_out = r->o.bp_minb > 0 ? r->o.bp_minb : 4;
+    return LCT_OK;
+  }
+  static std::mutex mu;
+  static std::map<std::vector<long long>, std::pair<int, int>> cache;
+  const std::vector<long long> key = {g.ns, g.nt, ig.nx, ig.ny, g.n_angle, g.n_proj_turn,
+                                      r->o.interp, (long long)(1000.0 * g.pitch / ig.dz),
+                                      (long long)r->info.n_blocks_run};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      r->o.bp_nz = it->second.first;
+      r->o.bp_minb = it->second.second;
+      if (nz_out) *nz_out = r->o.bp_nz;
+      if (minb_out) *minb_out = r->o.bp_minb;
+      return LCT_OK;
+    }
+  }
+  cudaStream_t s;
+  int st = cuda_status(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  if (st) return st;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const size_t qbytes = sizeof(float4) * (size_t)r->g_count * quad_view_elems(g.ns, g.nt);
+  st = cuda_status(cudaMemsetAsync(r->d_quad, 0, qbytes, s));
+  float best = 1e30f;
+  int bnz = 8, bmb = 4;
+  const int nzs[3] = {4, 8, 16}, mbs[3] = {2, 3, 4};
+  for (int i = 0; i < 3 && !st; ++i)
+    for (int j = 0; j < 3 && !st; ++j) {
+      r->o.bp_nz = nzs[i];
+      r->o.bp_minb = mbs[j];
+      if ((st = recon_stage_bp(r, r->d_img, s))) break;  // warm
+      cudaEventRecord(e0, s);
+      if ((st = recon_stage_bp(r, r->d_img, s))) break;
+      cudaEventRecord(e1, s);
+      if ((st = cuda_status(cudaEventSynchronize(e1)))) break;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) {
+        best = ms;
+        bnz = nzs[i];
+        bmb = mbs[j];
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(s);
+  r->o.bp_nz = bnz;
+  r->o.bp_minb = bmb;
+  if (st) return st;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = {bnz, bmb};
+  }
+  if (nz_out) *nz_out = bnz;
+  if (minb_out) *minb_out = bmb;
   return LCT_OK;
 }
 
@@ -239,12 +299,170 @@ static int run_filter(lct_recon* r, const lct_geom& g, long long nrows, cudaStre
   return launch_filter_rows(g.ns, r->d_h, r->d_par, nrows, LCT_FILTER_FP32, s);
 }
 
+// Block mode: the reference's per-block flow, every stage per block.
+static int run_blocks(lct_recon* r, const float* d_fan, float* d_img, cudaStream_t s) {
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  const int bp_nz = pick_bp_nz(g, ig, r->o.bp_nz);
+  int st;
+  for (int b = 0; b < r->info.n_blocks_run; ++b) {
+    const lct_block_info& bi = r->blocks[b];
+    const int addr = block_addr(r, b);
+    const float* fan_block = d_fan + (bi.block_proj_start - r->fan_first) * r->plane;
+    if ((st = run_rebin(r, g, fan_block, r->d_par, addr, s))) return st;
+    r->launches++;
+    if (r->o.preweight == LCT_PW_PI_ORI) {
+      if ((st = lct_weight_pi_ori(&g, r->d_par, s))) return st;
+      r->launches++;
+    }
+    if ((st = run_filter(r, g, (long long)g.n_angle * g.nt, s))) return st;
+    r->launches += filter_launches(r->o.filter_mode);
+    const float* betas = r->d_betas + bi.block_proj_start + g.add_projections;
+    float* img_b = d_img + (long long)b * slab;
+    if (r->o.backprojector == LCT_BP_PI_ORI) {
+      st = lct_backproject_pi_ori(&g, &ig, betas, r->d_par, img_b, r->o.interp, addr, s);
+    } else {
+      BpLaunch L;
+      L.proj = r->d_par;
+      L.betas = betas;
+      L.img = img_b;
+      L.view_stride = r->plane;
+      L.n_angle = g.n_angle;
+      L.nz = kBlockSlices;
+      L.n_slabs = 1;
+      L.slab_view[0] = 0;
+      L.slab_z0[0] = 0;
+      L.interp = r->o.interp;
+      L.addr = addr;
+      L.nz_thread = bp_nz;
+      L.minb = r->o.bp_minb;
+      if (r->quads) {
+        if ((st = launch_quad_pack(r->d_par, g.n_angle, g.ns, g.nt, addr, r->d_quad, s))) return st;
+        r->launches++;
+        st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
+      } else {
+        st = launch_bp_par(g, ig, L, s);
+      }
+    }
+    if (st) return st;
+    r->launches++;
+  }
+  return LCT_OK;
+}
+
+namespace lct {
+
+// Scan mode, stage 1: rebin every global view once (FP64 per-column shifts), pre-weight.
+int recon_stage_rebin(lct_recon* r, const float* d_fan, cudaStream_t s) {
+  const lct_geom& g = r->info.ctg;
+  const int addr0 = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  int st;
+  if (r->o.rebinner == LCT_REBIN_NULL) {
+    lct_geom gg = g;
+    gg.n_angle = (int)r->g_count;
+    gg.n_angle_add = (int)r->fan_count;
+    if ((st = lct_rebin_null(&gg, d_fan, r->d_par, addr0, s))) return st;
+  } else {
+    if ((st = launch_rebin_fan2par_scan(g, d_fan, r->fan_first, r->fan_count, r->d_par,
+                                        r->g_first, r->g_count, r->o.interp, addr0, s)))
+      return st;
+  }
+  r->launches++;
+  if (r->o.preweight == LCT_PW_PI_ORI) {
+    lct_geom gg = g;
+    gg.n_angle = (int)r->g_count;
+    gg.n_angle_add = (int)r->g_count;
+    if ((st = lct_weight_pi_ori(&gg, r->d_par, s))) return st;
+    r->launches++;
+  }
+  return LCT_OK;
+}
+
+// Scan mode, stage 2: filter every rebinned view once, pack the backprojector's quads.
+int recon_stage_filter(lct_recon* r, cudaStream_t s) {
+  const lct_geom& g = r->info.ctg;
+  int st;
+  if ((st = run_filter(r, g, r->g_count * g.nt, s))) return st;
+  r->launches += filter_launches(r->o.filter_mode);
+  if (r->quads && r->o.backprojector == LCT_BP_PAR) {
+    // border-addressed quads; a clamped (legacy first) slab reads the FP32 views directly
+    const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+    if ((st = launch_quad_pack(r->d_par, r->g_count, g.ns, g.nt, packed, r->d_quad, s))) return st;
+    r->launches++;
+  }
+  return LCT_OK;
+}
+
+// Scan mode, stage 3: the launch description of the slabs [b0, b1) (one addressing mode).
+void recon_bp_launch(const lct_recon* r, int b0, int b1, float* d_img, BpLaunch& L) {
+  const lct_geom& g = r->info.ctg;
+  L.proj = r->d_par;
+  L.img = d_img;
+  L.view_stride = r->plane;
+  L.n_angle = g.n_angle;
+  L.nz = kBlockSlices;
+  L.n_slabs = b1 - b0;
+  for (int b = b0; b < b1; ++b) {
+    const long long gv = r->blocks[b].block_proj_start + g.add_projections;
+    L.slab_view[b - b0] = (int)(gv - r->g_first);
+    L.slab_z0[b - b0] = b * kBlockSlices;
+  }
+  L.interp = r->o.interp;
+  L.addr = block_addr(r, b0);
+  L.nz_thread = pick_bp_nz(g, r->info.ig, r->o.bp_nz);
+  L.minb = r->o.bp_minb;
+  // betas are indexed by the same slab offset: shift the base by g_first
+  L.betas = r->d_betas + r->g_first;
+}
+
+bool recon_bp_quads_all(const lct_recon* r) {
+  return r->quads && r->o.backprojector == LCT_BP_PAR && r->o.addr != LCT_ADDR_LEGACY;
+}
+
+int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s) {
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  const int nb = r->info.n_blocks_run;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  int st;
+  if (r->o.backprojector == LCT_BP_PI_ORI) {
+    for (int b = 0; b < nb; ++b) {
+      const long long gv = r->blocks[b].block_proj_start + g.add_projections;
+      st = lct_backproject_pi_ori(&g, &ig, r->d_betas + gv, r->d_par + (gv - r->g_first) * r->plane,
+                                  d_img + (long long)b * slab, r->o.interp, block_addr(r, b), s);
+      if (st) return st;
+      r->launches++;
+    }
+    return LCT_OK;
+  }
+  // one launch over every slab; with LEGACY addressing slab 0 runs apart (clamped)
+  int b0 = 0;
+  while (b0 < nb) {
+    const int addr = block_addr(r, b0);
+    int b1 = b0 + 1;
+    while (b1 < nb && block_addr(r, b1) == addr) ++b1;
+    BpLaunch L;
+    recon_bp_launch(r, b0, b1, d_img, L);
+    const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+    if (r->quads && addr == packed)
+      st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
+    else
+      st = launch_bp_par(g, ig, L, s);
+    if (st) return st;
+    r->launches++;
+    b0 = b1;
+  }
+  return LCT_OK;
+}
+
+}  // namespace lct
+
 LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                           float* image, int image_on_device, lct_stream stream) {
   if (!r || !fan || !image) return LCT_ERR_ARG;
   if (fan_view0 < 0 || fan_view0 > r->fan_first + r->info.data_offset) return LCT_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
-  const lct_geom& g = r->info.ctg;
   const lct_img& ig = r->info.ig;
   const int nb = r->info.n_blocks_run;
   const long long off = r->info.data_offset;
@@ -267,134 +485,19 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
   if ((st = cuda_status(cudaEventRecord(r->ev[1], s)))) return st;
   float* d_img = image_on_device ? image : r->d_img;
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
-  const int bp_nz = pick_bp_nz(g, ig, r->o.bp_nz);
 
   if (r->o.mode == LCT_MODE_BLOCK) {
     // stages interleave per block; the whole compute span is reported as backprojection
     cudaEventRecord(r->ev[2], s);
     cudaEventRecord(r->ev[3], s);
-    for (int b = 0; b < nb; ++b) {
-      const lct_block_info& bi = r->blocks[b];
-      const int addr = block_addr(r, b);
-      const float* fan_block = d_fan + (bi.block_proj_start - r->fan_first) * r->plane;
-      if ((st = run_rebin(r, g, fan_block, r->d_par, addr, s))) return st;
-      r->launches++;
-      if (r->o.preweight == LCT_PW_PI_ORI) {
-        if ((st = lct_weight_pi_ori(&g, r->d_par, s))) return st;
-        r->launches++;
-      }
-      if ((st = run_filter(r, g, (long long)g.n_angle * g.nt, s))) return st;
-      r->launches += filter_launches(r->o.filter_mode);
-      const float* betas = r->d_betas + bi.block_proj_start + g.add_projections;
-      float* img_b = d_img + (long long)b * slab;
-      if (r->o.backprojector == LCT_BP_PI_ORI) {
-        st = lct_backproject_pi_ori(&g, &ig, betas, r->d_par, img_b, r->o.interp, addr, s);
-      } else {
-        BpLaunch L;
-        L.proj = r->d_par;
-        L.betas = betas;
-        L.img = img_b;
-        L.view_stride = r->plane;
-        L.n_angle = g.n_angle;
-        L.nz = kBlockSlices;
-        L.n_slabs = 1;
-        L.slab_view[0] = 0;
-        L.slab_z0[0] = 0;
-        L.interp = r->o.interp;
-        L.addr = addr;
-        L.nz_thread = bp_nz;
-        L.minb = r->o.bp_minb;
-        if (r->quads) {
-          if ((st = launch_quad_pack(r->d_par, g.n_angle, g.ns, g.nt, addr, r->d_quad, s))) return st;
-          r->launches++;
-          st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
-        } else {
-          st = launch_bp_par(g, ig, L, s);
-        }
-      }
-      if (st) return st;
-      r->launches++;
-    }
+    if ((st = run_blocks(r, d_fan, d_img, s))) return st;
     cudaEventRecord(r->ev[4], s);
   } else {
-    // scan mode: rebin every global view once (FP64 per-column shifts), filter once
-    const long long fan_base = r->fan_first;  // d_fan view 0 == global fan view fan_first
-    const int addr0 = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
-    if (r->o.rebinner == LCT_REBIN_NULL) {
-      lct_geom gg = g;
-      gg.n_angle = (int)r->g_count;
-      gg.n_angle_add = (int)r->fan_count;
-      if ((st = lct_rebin_null(&gg, d_fan, r->d_par, addr0, s))) return st;
-    } else {
-      if ((st = launch_rebin_fan2par_scan(g, d_fan, fan_base, r->fan_count, r->d_par, r->g_first,
-                                          r->g_count, r->o.interp, addr0, s)))
-        return st;
-    }
-    r->launches++;
-    if (r->o.preweight == LCT_PW_PI_ORI) {
-      lct_geom gg = g;
-      gg.n_angle = (int)r->g_count;
-      gg.n_angle_add = (int)r->g_count;
-      if ((st = lct_weight_pi_ori(&gg, r->d_par, s))) return st;
-      r->launches++;
-    }
+    if ((st = recon_stage_rebin(r, d_fan, s))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[2], s)))) return st;
-    if ((st = run_filter(r, g, r->g_count * g.nt, s))) return st;
-    r->launches += filter_launches(r->o.filter_mode);
-    if (r->quads && r->o.backprojector == LCT_BP_PAR) {
-      // border-addressed quads; a clamped (legacy first) slab reads the FP32 views directly
-      if ((st = launch_quad_pack(r->d_par, r->g_count, g.ns, g.nt, LCT_ADDR_CLAMP == r->o.addr
-                                                                      ? LCT_ADDR_CLAMP
-                                                                      : LCT_ADDR_BORDER,
-                                 r->d_quad, s)))
-        return st;
-      r->launches++;
-    }
+    if ((st = recon_stage_filter(r, s))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[3], s)))) return st;
-    if (r->o.backprojector == LCT_BP_PI_ORI) {
-      for (int b = 0; b < nb; ++b) {
-        const long long gv = r->blocks[b].block_proj_start + g.add_projections;
-        st = lct_backproject_pi_ori(&g, &ig, r->d_betas + gv, r->d_par + (gv - r->g_first) * r->plane,
-                                    d_img + (long long)b * slab, r->o.interp, block_addr(r, b), s);
-        if (st) return st;
-        r->launches++;
-      }
-    } else {
-      // one launch over every slab; with LEGACY addressing slab 0 runs apart (clamped)
-      int b0 = 0;
-      while (b0 < nb) {
-        const int addr = block_addr(r, b0);
-        int b1 = b0 + 1;
-        while (b1 < nb && block_addr(r, b1) == addr) ++b1;
-        BpLaunch L;
-        L.proj = r->d_par;
-        L.betas = r->d_betas;
-        L.img = d_img;
-        L.view_stride = r->plane;
-        L.n_angle = g.n_angle;
-        L.nz = kBlockSlices;
-        L.n_slabs = b1 - b0;
-        for (int b = b0; b < b1; ++b) {
-          const long long gv = r->blocks[b].block_proj_start + g.add_projections;
-          L.slab_view[b - b0] = (int)(gv - r->g_first);
-          L.slab_z0[b - b0] = b * kBlockSlices;
-        }
-        L.interp = r->o.interp;
-        L.addr = addr;
-        L.nz_thread = bp_nz;
-        L.minb = r->o.bp_minb;
-        // betas are indexed by the same slab offset: shift the base by g_first
-        L.betas = r->d_betas + r->g_first;
-        const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
-        if (r->quads && addr == packed)
-          st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
-        else
-          st = launch_bp_par(g, ig, L, s);
-        if (st) return st;
-        r->launches++;
-        b0 = b1;
-      }
-    }
+    if ((st = recon_stage_bp(r, d_img, s))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
   }
 

@@ -1,0 +1,38 @@
+// lct_recon internals shared by recon.cu and batch.cu (not part of the ABI).
+#pragma once
+
+#include <vector>
+
+#include "lct_internal.h"
+
+struct lct_recon {
+  lct_plan_info info;
+  std::vector<lct_block_info> blocks;
+  lct_recon_opts o;
+  long long plane = 0;           // nt * ns
+  long long fan_first = 0, fan_count = 0;
+  long long g_first = 0, g_count = 0;  // scan mode
+  float* d_fan = nullptr;
+  float* d_par = nullptr;
+  float* d_betas = nullptr;
+  float* d_h = nullptr;
+  float* d_img = nullptr;
+  float4* d_quad = nullptr;  // filtered views in quad layout (backprojection input)
+  void* d_tc = nullptr;      // BF16x3 filter operands (row and Toeplitz planes)
+  long long tc_rows = 0;
+  bool quads = false;        // full windows: the quad-layout pairs kernel applies
+  cudaEvent_t ev[6] = {};
+  float times[5] = {};
+  int device = 0;
+  long long voxel_updates = 0;
+  int launches = 0;
+};
+
+namespace lct {
+// scan-mode stages of one recon, on any stream (used by lct_recon_run and the batch graphs)
+int recon_stage_rebin(lct_recon* r, const float* d_fan, cudaStream_t s);
+int recon_stage_filter(lct_recon* r, cudaStream_t s);
+int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s);
+void recon_bp_launch(const lct_recon* r, int b0, int b1, float* d_img, BpLaunch& L);
+bool recon_bp_quads_all(const lct_recon* r);
+}  // namespace lct

@@ -129,6 +129,11 @@ class Reconstruction:
         capi.check(self._lib.lct_recon_stats_get(self._h, C.byref(st)))
         return st
 
+    def autotune(self) -> tuple[int, int]:
+        nz, mb = C.c_int(), C.c_int()
+        capi.check(self._lib.lct_recon_autotune(self._h, C.byref(nz), C.byref(mb)))
+        return nz.value, mb.value
+
     def last_times(self) -> dict:
         t = (C.c_float * 5)()
         capi.check(self._lib.lct_recon_last_times(self._h, t))
@@ -138,6 +143,61 @@ class Reconstruction:
         h = getattr(self, "_h", None)
         if h:
             self._lib.lct_recon_destroy(h)
+            self._h = None
+
+
+class Batch:
+    """lct_batch: many independent scans reconstructed together -- one CUDA-graph launch per
+    stage, one persistent work-list backprojection over all scans' tiles."""
+
+    def __init__(self, plans: list[Plan], **opts):
+        self._lib = capi.load()
+        self.plans = list(plans)
+        self.opts = recon_opts(**opts)
+        arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
+        h = C.c_void_p()
+        capi.check(self._lib.lct_batch_create(arr, len(plans), C.byref(self.opts), C.byref(h)),
+                   "lct_batch_create")
+        self._h = h
+        self.fan_ranges = []
+        for i in range(len(plans)):
+            f, c = C.c_int64(), C.c_int64()
+            capi.check(self._lib.lct_batch_fan_range(h, i, C.byref(f), C.byref(c)))
+            self.fan_ranges.append((f.value, c.value))
+        self.image_shapes = [(p.info.n_blocks_run * BLOCK_SLICES, p.info.ig.ny, p.info.ig.nx)
+                             for p in plans]
+
+    def run(self, fans, images=None, fan_view0=None, stream=None):
+        torch = _torch()
+        n = len(self.plans)
+        if images is None:
+            images = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in self.image_shapes]
+        fp = [_ptr(f) for f in fans]
+        ip = [_ptr(i) for i in images]
+        if len({d for d, _ in fp}) != 1 or len({d for d, _ in ip}) != 1:
+            raise ValueError("all fans (and all images) must be on the same side")
+        v0 = (C.c_int64 * n)(*(fan_view0 or [0] * n))
+        fa = (C.c_void_p * n)(*[p for _, p in fp])
+        ia = (C.c_void_p * n)(*[p for _, p in ip])
+        s = stream if stream is not None else _stream()
+        capi.check(self._lib.lct_batch_run(self._h, fa, v0, int(fp[0][0]), ia, int(ip[0][0]), s),
+                   "lct_batch_run")
+        return images
+
+    def stats(self) -> capi.ReconStats:
+        st = capi.ReconStats()
+        capi.check(self._lib.lct_batch_stats_get(self._h, C.byref(st)))
+        return st
+
+    def last_times(self) -> dict:
+        t = (C.c_float * 5)()
+        capi.check(self._lib.lct_batch_last_times(self._h, t))
+        return dict(zip(["upload", "rebin", "filter", "backproject", "download"], list(t)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.lct_batch_destroy(h)
             self._h = None
 
 
