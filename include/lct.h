@@ -305,6 +305,60 @@ int lct_sim_project(const double* d_ellipsoids, int n_ellipsoids, int ns, int nt
                     const double* d_zpos, int64_t v0, int64_t v1, double i0, uint64_t seed,
                     float* d_fan, lct_stream stream);
 
+/* Voxelised phantom on the GPU (training targets): mean attenuation over ss^3 sub-samples per
+   voxel, d_out [nz][ny][nx], voxel (ix, iy, iz) centred at (x0 + ix dx, y0 + iy dy, z0 + iz dz).
+   Asynchronous. */
+int lct_voxelise(const double* d_ellipsoids, int n_ellipsoids, int nx, int ny, int nz, double x0,
+                 double y0, double z0, double dx, double dy, double dz, int ss, float* d_out,
+                 lct_stream stream);
+
+/* ---------------------------------------------------------------------------------------
+ * Learned 2.5D residual correction (no reference counterpart: the reference stops at the FDK
+ * volume).  5 neighbouring slices of the calibrated FDK volume in, 8 zero-padded 3x3
+ * convolutions (5->32, 6 x 32->32, 32->1) with ReLU between them, a residual r out:
+ *   plain(z)     = calib * fdk(z)                       (calibrated plain FDK, phantom units)
+ *   network in   = bf16(calib * in_scale * fdk(z-2..z+2))
+ *   corrected(z) = plain(z) + r / in_scale   where |r / in_scale| <= bound, else plain(z)
+ * BF16 weights and activations, FP32 accumulation, tcgen05 implicit-GEMM convolutions.
+ * Parameters: 57,249 floats, for l = 0..7: W_l[cout][cin][3][3], then b_l[cout]
+ * (FP32 master copy; Adam state on the device).
+ * ------------------------------------------------------------------------------------- */
+#define LCT_CNN_TRAIN 1 /* keep every activation and the deltas (training); else inference only */
+typedef struct lct_cnn lct_cnn;
+int lct_cnn_param_count(int64_t* n);
+/* Workspace for up to max_slices slices of ny x nx; weights He-initialised from seed.
+   Synchronous. */
+int lct_cnn_create(int max_slices, int ny, int nx, int flags, uint64_t seed, lct_cnn** out);
+/* Parameter copies (host or device pointers, synchronous).  set_params resets the Adam state. */
+int lct_cnn_set_params(lct_cnn* c, const float* params, int on_device);
+int lct_cnn_get_params(const lct_cnn* c, float* params, int on_device);
+int lct_cnn_get_grads(const lct_cnn* c, float* grads, int on_device);
+int lct_cnn_set_scales(lct_cnn* c, float calib, float in_scale);
+int lct_cnn_get_scales(const lct_cnn* c, float* calib, float* in_scale);
+/* Training (LCT_CNN_TRAIN workspaces).  d_in5 [n][5][ny][nx]: FDK slices z-2..z+2 (raw FDK
+   units); d_target [n][ny][nx]: phantom slices (phantom units).  forward writes the residual r
+   (network units) to d_resid when non-null; backward (after forward on the same inputs)
+   computes the gradient of mean((in_scale*plain + r - in_scale*target)^2); adam_step updates
+   the FP32 master weights; train_step = forward + backward + adam_step(0.9, 0.999, 1e-8).
+   Asynchronous on the stream. */
+int lct_cnn_forward(lct_cnn* c, const float* d_in5, int n_slices, float* d_resid,
+                    lct_stream stream);
+int lct_cnn_backward(lct_cnn* c, const float* d_in5, const float* d_target, int n_slices,
+                     lct_stream stream);
+int lct_cnn_adam_step(lct_cnn* c, float lr, float beta1, float beta2, float eps,
+                      lct_stream stream);
+int lct_cnn_train_step(lct_cnn* c, const float* d_in5, const float* d_target, int n_slices,
+                       float lr, lct_stream stream);
+/* loss of the last backward pass (synchronous) */
+int lct_cnn_last_loss(const lct_cnn* c, double* loss);
+/* Inference with the acceptance gate over a device volume d_vol [nz][ny][nx] (raw FDK) ->
+   d_out (corrected, phantom units; must not alias d_vol), max_slices slices per pass, edge
+   slices replicated.  n_rejected (host, may be NULL): voxels where the gate kept the plain
+   value; when given, the call synchronises the stream. */
+int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, int nz, float bound,
+                         int64_t* n_rejected, lct_stream stream);
+void lct_cnn_destroy(lct_cnn* c);
+
 /* ---------------------------------------------------------------------------------------
  * Diagnostics
  * ------------------------------------------------------------------------------------- */

@@ -123,6 +123,8 @@ GP = C.POINTER(Geom)
 IP = C.POINTER(Img)
 
 # name -> (restype, argtypes); every symbol include/lct.h declares
+CNN_TRAIN = 1
+
 SIGNATURES: dict[str, tuple] = {
     "lct_status_string": (C.c_char_p, [I32]),
     "lct_last_cuda_error": (I32, []),
@@ -158,6 +160,21 @@ SIGNATURES: dict[str, tuple] = {
     "lct_batch_destroy": (None, [P]),
     "lct_sim_project": (I32, [P, I32, I32, I32, F32, F32, F32, F32, F32, P, P, I64, I64, F64, U64, P, P]),
     "lct_diag_tex3d_sample": (I32, [P, I32, I32, I32, P, I64, I32, P]),
+    "lct_voxelise": (I32, [P, I32, I32, I32, I32, F64, F64, F64, F64, F64, F64, I32, P, P]),
+    "lct_cnn_param_count": (I32, [P]),
+    "lct_cnn_create": (I32, [I32, I32, I32, I32, U64, P]),
+    "lct_cnn_set_params": (I32, [P, P, I32]),
+    "lct_cnn_get_params": (I32, [P, P, I32]),
+    "lct_cnn_get_grads": (I32, [P, P, I32]),
+    "lct_cnn_set_scales": (I32, [P, F32, F32]),
+    "lct_cnn_get_scales": (I32, [P, P, P]),
+    "lct_cnn_forward": (I32, [P, P, I32, P, P]),
+    "lct_cnn_backward": (I32, [P, P, P, I32, P]),
+    "lct_cnn_adam_step": (I32, [P, F32, F32, F32, F32, P]),
+    "lct_cnn_train_step": (I32, [P, P, P, I32, F32, P]),
+    "lct_cnn_last_loss": (I32, [P, P]),
+    "lct_cnn_infer_volume": (I32, [P, P, P, I32, F32, P, P]),
+    "lct_cnn_destroy": (None, [P]),
 }
 
 _lib: C.CDLL | None = None

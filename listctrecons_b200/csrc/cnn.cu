@@ -1,0 +1,821 @@
+// Learned 2.5D residual correction after backprojection (no reference counterpart; the
+// reference stops at the FDK volume, Src/Reconstructor.cpp).
+//
+// Network: 5 neighbouring slices of the (calibrated) FDK volume as channels -> 8 zero-padded
+// 3x3 convolutions (5->32, 6 x 32->32, 32->1), ReLU between them -> a residual r added to the
+// centre slice.  BF16 weights and activations, FP32 accumulation.
+//
+// HBM layout: every activation / delta is channels-last bf16 [B][H][W+2][32] (64 bytes per
+// pixel; one zero pad column on each side, pixel x at column x+1; channels beyond a layer's
+// width are zero).  Weights are packed per layer as bf16 [N][9 taps x 32 channels].
+//
+// Convolution = implicit GEMM on tcgen05: a CTA computes 128 consecutive pixels of one image
+// row x N output channels (N = 32, or 16 for the 1-channel last layer) over K = 9 taps x 32
+// channels.  Per tap, one 4-D TMA box {32 ch, 128 px, 1 row, 1 slice} with 64-byte swizzle
+// lands in a 4-stage ring (rows above/below the image come back as TMA's zero fill); the
+// packed weights (9 x N x 64 bytes) sit in shared memory; two M128 x N x K16 MMAs per tap
+// accumulate in TMEM.  Fused epilogues: bias + ReLU -> bf16 (forward), ReLU mask of the
+// previous activation -> bf16 delta (backward data), FP32 residual (training), and the
+// acceptance gate writing the corrected volume (inference).
+// Weight gradients: SIMT FP32 outer products over row segments staged in shared memory.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <new>
+#include <vector>
+
+#include "lct_internal.h"
+#include "tc_ptx.cuh"
+
+namespace lct {
+
+constexpr int kCnnLayers = 8, kCnnC = 32, kCnnTaps = 9, kCnnK = kCnnTaps * kCnnC;  // K = 288
+constexpr int kCnnParams = 57249;     // sum over layers of cin*cout*9 + cout
+constexpr int kConvM = 128, kConvStages = 4, kConvThreads = 128;
+constexpr int kWSlot = kCnnC * kCnnK;  // packed weights of one layer, elements
+
+LCT_HD constexpr int cnn_cin(int l) { return l == 0 ? 5 : 32; }
+LCT_HD constexpr int cnn_cout(int l) { return l == kCnnLayers - 1 ? 1 : 32; }
+LCT_HD constexpr int cnn_off(int l) { return l == 0 ? 0 : 1472 + (l - 1) * 9248; }
+
+enum ConvEpi : int { kEpiRelu = 0, kEpiMask = 1, kEpiResid = 2, kEpiGate = 3 };
+
+struct ConvArgs {
+  int H, W, wp, tiles_x;
+  const float* bias;               // [N] (forward epilogues)
+  __nv_bfloat16* out_act;          // Relu / Mask: [B][H][wp][32]
+  const __nv_bfloat16* mask_act;   // Mask: activation whose sign gates the delta
+  float* out_f;                    // Resid: r [B][H][W]; Gate: corrected slices [B][H][W]
+  const float* xc;                 // Gate: plain slices [B][H][W]
+  float calib, inv_scale, bound;   // Gate
+  unsigned long long* n_reject;    // Gate
+  int* status;
+};
+
+template <int N>
+struct ConvCfg {
+  static constexpr uint32_t TileA = kConvM * kCnnC * 2;  // 8 KB per tap
+  static constexpr uint32_t TapB = N * kCnnC * 2;        // 2 KB (N=32) or 1 KB (N=16)
+  static constexpr uint32_t BBytes = kCnnTaps * TapB;
+  static constexpr uint32_t Smem = 1024 + kConvStages * TileA + BBytes + 128;
+  static constexpr uint32_t TmemCols = 32;
+  static constexpr uint32_t Idesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                                    ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kConvM >> 4) << 24);
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+
+template <int N, int EPI>
+__global__ void __launch_bounds__(kConvThreads, 4)
+    conv_tc_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
+                   const ConvArgs a) {
+  using Cfg = ConvCfg<N>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint8_t* sa = smem;
+  uint8_t* sb = smem + kConvStages * Cfg::TileA;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sb + Cfg::BBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kConvStages + 2);
+  __shared__ int s_abort;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x;
+  const int xt = t % a.tiles_x, q = t / a.tiles_x;
+  const int y = q % a.H, b = q / a.H;
+  const int x0 = xt * kConvM;
+  const uint32_t full0 = smem_u32(&bars[0]);
+  const uint32_t empty0 = smem_u32(&bars[kConvStages]);
+  const uint32_t wbar = smem_u32(&bars[2 * kConvStages]);
+  const uint32_t accum = smem_u32(&bars[2 * kConvStages + 1]);
+
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < kConvStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(wbar, 1);
+    mbar_init(accum, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(Cfg::TmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // producer: the layer's packed weights once, then one A box per tap
+    mbar_expect_tx(wbar, Cfg::BBytes);
+    for (int k = 0; k < kCnnTaps; ++k)
+      tma_load_2d(smem_u32(sb + k * Cfg::TapB), &mw, k * kCnnC, 0, wbar);
+    int issued = 0;
+    for (int k = 0; k < kCnnTaps; ++k) {
+      const int s = k % kConvStages;
+      if (k >= kConvStages && !mbar_wait(empty0 + 8 * s, ((k / kConvStages) - 1) & 1)) {
+        atomicExch(&s_abort, 1);
+        break;
+      }
+      if (atomicAdd(&s_abort, 0)) break;
+      const int dy = k / 3 - 1, dx = k % 3 - 1;
+      mbar_expect_tx(full0 + 8 * s, Cfg::TileA);
+      // pixel x of the tile reads column x + 1 + dx of the padded rows
+      tma_load_4d(smem_u32(sa + s * Cfg::TileA), &mx, 0, x0 + 1 + dx, y + dy, b, full0 + 8 * s);
+      issued = k + 1;
+    }
+    if (atomicAdd(&s_abort, 0)) {  // let copies in flight land before the CTA exits
+      mbar_wait(wbar, 0);
+      for (int k = (issued > kConvStages ? issued - kConvStages : 0); k < issued; ++k)
+        mbar_wait(full0 + 8 * (k % kConvStages), (k / kConvStages) & 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    if (!mbar_wait(wbar, 0)) {
+      atomicExch(&s_abort, 1);
+    } else {
+      for (int k = 0; k < kCnnTaps; ++k) {
+        const int s = k % kConvStages;
+        if (!mbar_wait(full0 + 8 * s, (k / kConvStages) & 1)) {
+          atomicExch(&s_abort, 1);
+          break;
+        }
+        tc_fence_after();
+        const uint64_t da = desc_sw64(smem_u32(sa + s * Cfg::TileA));
+        const uint64_t db = desc_sw64(smem_u32(sb + k * Cfg::TapB));
+        umma_bf16(tmem, da, db, Cfg::Idesc, k ? 1u : 0u);
+        umma_bf16(tmem, da + 2, db + 2, Cfg::Idesc, 1u);  // +32 bytes: channels 16..31
+        umma_commit(empty0 + 8 * s);
+      }
+    }
+    umma_commit(accum);
+  }
+  __syncwarp();
+
+  const bool done = mbar_wait(accum, 0);
+  __syncthreads();
+  tc_fence_after();
+  const bool ok = done && !*reinterpret_cast<volatile int*>(&s_abort);
+  if (!ok) {
+    if (threadIdx.x == 0 && a.status) atomicExch(a.status, kDevWaitTimeout);
+  } else {
+    const int i = warp * 32 + lane;
+    const int x = x0 + i;
+    const bool in = x < a.W;
+    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16);
+    if constexpr (N == 32) {
+      uint32_t r[32];
+      tmem_ld32(ta, r);
+      if (in) {
+        const long long pix = ((long long)b * a.H + y) * a.wp + x + 1;
+        uint4* dst = reinterpret_cast<uint4*>(a.out_act + pix * kCnnC);
+        if constexpr (EPI == kEpiRelu) {
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              v[j] = fmaxf(__uint_as_float(r[8 * g + j]) + __ldg(a.bias + 8 * g + j), 0.f);
+            dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
+                                pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+          }
+        } else {
+          const uint4* msk = reinterpret_cast<const uint4*>(a.mask_act + pix * kCnnC);
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            const uint4 mv = msk[g];
+            const uint32_t mwd[4] = {mv.x, mv.y, mv.z, mv.w};
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int16_t bits = (int16_t)((mwd[j >> 1] >> (16 * (j & 1))) & 0xFFFFu);
+              v[j] = bits > 0 ? __uint_as_float(r[8 * g + j]) : 0.f;
+            }
+            dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
+                                pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+          }
+        }
+      }
+    } else {
+      uint32_t r[16];
+      tmem_ld16(ta, r);
+      const long long o = ((long long)b * a.H + y) * a.W + x;
+      const float rr = __uint_as_float(r[0]) + __ldg(a.bias);
+      if constexpr (EPI == kEpiResid) {
+        if (in) a.out_f[o] = rr;
+      } else {
+        bool rej = false;
+        if (in) {
+          const float plain = a.calib * a.xc[o];
+          const float d = rr * a.inv_scale;
+          const bool keep = fabsf(d) <= a.bound;  // NaN fails the test: plain is kept
+          a.out_f[o] = keep ? plain + d : plain;
+          rej = !keep;
+        }
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, rej);
+        if (lane == 0 && m && a.n_reject) atomicAdd(a.n_reject, (unsigned long long)__popc(m));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(Cfg::TmemCols)
+                 : "memory");
+}
+
+// Network input: channel k of slice b = k_in * plane(b, k), k < 5; pads and channels >= 5 zero.
+// plane(b, k) = b*5 + k for stacked training inputs [B][5][H][W], or the volume slice
+// clamp(z0 + b + k - 2, 0, nz - 1) for inference over a volume [nz][H][W].
+__global__ void cnn_prep_kernel(const float* __restrict__ src, int vol_mode, int z0, int nz,
+                                int B, int H, int W, int wp, float k_in,
+                                __nv_bfloat16* __restrict__ a0) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)B * H * wp) return;
+  const int col = (int)(i % wp);
+  const long long q = i / wp;
+  const int y = (int)(q % H), b = (int)(q / H), x = col - 1;
+  float v[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  if (x >= 0 && x < W) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      long long plane;
+      if (vol_mode) {
+        int z = z0 + b + k - 2;
+        z = z < 0 ? 0 : (z > nz - 1 ? nz - 1 : z);
+        plane = z;
+      } else {
+        plane = (long long)b * 5 + k;
+      }
+      v[k] = __fmul_rn(k_in, src[(plane * H + y) * W + x]);
+    }
+  }
+  uint4* dst = reinterpret_cast<uint4*>(a0 + i * kCnnC);
+  dst[0] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], 0.f), 0u);
+  dst[1] = make_uint4(0u, 0u, 0u, 0u);
+  dst[2] = make_uint4(0u, 0u, 0u, 0u);
+  dst[3] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// MSE loss of (k_in x_c + r) against s t and its gradient 2 d / n -> channel 0 of the last
+// layer's delta (bf16, padded layout); sum of d^2 accumulated in FP64.
+__global__ void __launch_bounds__(256) cnn_loss_kernel(const float* __restrict__ in5,
+                                                       const float* __restrict__ r,
+                                                       const float* __restrict__ tgt, int B,
+                                                       int H, int W, int wp, float k_in, float s,
+                                                       float two_over_n, __nv_bfloat16* dz,
+                                                       double* loss) {
+  __shared__ float red[8];
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long hw = (long long)H * W;
+  float d2 = 0.f;
+  if (p < B * hw) {
+    const long long b = p / hw, pix = p % hw;
+    const int y = (int)(pix / W), x = (int)(pix % W);
+    const float xc = in5[(b * 5 + 2) * hw + pix];
+    const float yv = __fadd_rn(__fmul_rn(k_in, xc), r[p]);
+    const float d = __fsub_rn(yv, __fmul_rn(s, tgt[p]));
+    d2 = d * d;
+    dz[((b * H + y) * wp + x + 1) * kCnnC] = __float2bfloat16_rn(__fmul_rn(d, two_over_n));
+  }
+  for (int o = 16; o; o >>= 1) d2 += __shfl_xor_sync(0xFFFFFFFFu, d2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = d2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += red[w];
+    atomicAdd(loss, sum);
+  }
+}
+
+// Weight / bias gradients of one layer: dW[co][ci][ky][kx] = sum_p dz[p][co] a[p + (ky-1, kx-1)][ci].
+// Segment = 64 pixels of one row; thread (ky, 4 co, 4 ci) keeps 4 x 4 x 3 FP32 partial sums over
+// the CTA's segments and adds them to the gradient once.
+constexpr int kDwSeg = 64, kDwThreads = 192;
+__global__ void __launch_bounds__(kDwThreads) cnn_dw_kernel(const __nv_bfloat16* __restrict__ act,
+                                                            const __nv_bfloat16* __restrict__ dz,
+                                                            int B, int H, int W, int wp, int cin,
+                                                            int cout, float* __restrict__ gw,
+                                                            float* __restrict__ gb) {
+  __shared__ __align__(16) __nv_bfloat16 s_a[3][kDwSeg + 2][kCnnC];
+  __shared__ __align__(16) __nv_bfloat16 s_d[kDwSeg][kCnnC];
+  const int t = threadIdx.x, ky = t / 64, rem = t % 64, cog = rem / 8, cig = rem % 8;
+  float acc[4][4][3];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[i][j][k] = 0.f;
+  float accb[4] = {0.f, 0.f, 0.f, 0.f};
+  const bool bias_thread = ky == 0 && cig == 0;
+  const int segs_x = (W + kDwSeg - 1) / kDwSeg;
+  const long long n_segs = (long long)B * H * segs_x;
+  for (long long sg = blockIdx.x; sg < n_segs; sg += gridDim.x) {
+    const int sx = (int)(sg % segs_x);
+    const long long q = sg / segs_x;
+    const int y = (int)(q % H), b = (int)(q / H), x0 = sx * kDwSeg;
+    __syncthreads();
+    for (int i = t; i < 3 * (kDwSeg + 2) * 4; i += kDwThreads) {
+      const int g = i & 3, px = (i >> 2) % (kDwSeg + 2), r = (i >> 2) / (kDwSeg + 2);
+      const int yy = y + r - 1, col = x0 + px;  // padded column
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (yy >= 0 && yy < H && col < wp)
+        v = reinterpret_cast<const uint4*>(act + (((long long)b * H + yy) * wp + col) * kCnnC)[g];
+      reinterpret_cast<uint4*>(&s_a[r][px][0])[g] = v;
+    }
+    for (int i = t; i < kDwSeg * 4; i += kDwThreads) {
+      const int g = i & 3, px = i >> 2, x = x0 + px;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (x < W)
+        v = reinterpret_cast<const uint4*>(dz + (((long long)b * H + y) * wp + x + 1) * kCnnC)[g];
+      reinterpret_cast<uint4*>(&s_d[px][0])[g] = v;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int p = 0; p < kDwSeg; ++p) {
+      const uint2 dv = *reinterpret_cast<const uint2*>(&s_d[p][cog * 4]);
+      const float d[4] = {bf16_lo(dv.x), bf16_hi(dv.x), bf16_lo(dv.y), bf16_hi(dv.y)};
+      if (bias_thread)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) accb[c] += d[c];
+#pragma unroll
+      for (int kx = 0; kx < 3; ++kx) {
+        const uint2 av = *reinterpret_cast<const uint2*>(&s_a[ky][p + kx][cig * 4]);
+        const float v[4] = {bf16_lo(av.x), bf16_hi(av.x), bf16_lo(av.y), bf16_hi(av.y)};
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[c][j][kx] = fmaf(d[c], v[j], acc[c][j][kx]);
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int co = cog * 4 + c;
+    if (co >= cout) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int ci = cig * 4 + j;
+      if (ci >= cin) continue;
+#pragma unroll
+      for (int kx = 0; kx < 3; ++kx)
+        atomicAdd(&gw[((co * cin + ci) * 3 + ky) * 3 + kx], acc[c][j][kx]);
+    }
+    if (bias_thread) atomicAdd(&gb[co], accb[c]);
+  }
+}
+
+__global__ void cnn_adam_kernel(float* __restrict__ p, const float* __restrict__ g,
+                                float* __restrict__ m, float* __restrict__ v, int n, float lr,
+                                float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+// FP32 master weights -> bf16 GEMM operands.  Forward slot l: [co][tap*32 + ci].  Backward
+// (data) slot l: [ci][tap*32 + co] holding W[co][ci][8 - tap] (the flipped, transposed kernel).
+__global__ void cnn_pack_kernel(const float* __restrict__ p, __nv_bfloat16* __restrict__ wf,
+                                __nv_bfloat16* __restrict__ wb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kCnnLayers * kWSlot) return;
+  const int l = i / kWSlot, rem = i % kWSlot, row = rem / kCnnK, k = rem % kCnnK;
+  const int tap = k / kCnnC, c = k % kCnnC;
+  const int cin = cnn_cin(l), cout = cnn_cout(l);
+  const float* w = p + cnn_off(l);
+  float f = 0.f, bwd = 0.f;
+  if (row < cout && c < cin) f = w[(row * cin + c) * 9 + tap];
+  if (l > 0 && row < cin && c < cout) bwd = w[(c * cin + row) * 9 + (8 - tap)];
+  wf[i] = __float2bfloat16_rn(f);
+  wb[i] = __float2bfloat16_rn(bwd);
+}
+
+}  // namespace lct
+
+using namespace lct;
+
+struct lct_cnn {
+  int device = 0, cap = 0, H = 0, W = 0, wp = 0, sms = 148;
+  bool train = false;
+  int n_act = 0;
+  long long act_elems = 0;
+  float* d_p = nullptr;  // params, grads, Adam m, Adam v: 4 x kCnnParams
+  float* d_g = nullptr;
+  float* d_m = nullptr;
+  float* d_v = nullptr;
+  __nv_bfloat16* d_wf = nullptr;  // 8 forward slots
+  __nv_bfloat16* d_wb = nullptr;  // 8 backward slots (slot 0 unused)
+  __nv_bfloat16* d_act = nullptr; // n_act activation buffers
+  __nv_bfloat16* d_dz = nullptr;  // training: 3 delta buffers
+  float* d_r = nullptr;           // training: residual [cap][H][W]
+  double* d_loss = nullptr;
+  unsigned long long* d_rej = nullptr;
+  CUtensorMap m_act[kCnnLayers], m_dz[3], m_wf[kCnnLayers], m_wb[kCnnLayers];
+  float calib = 1.f, in_scale = 1.f;
+  int adam_t = 0;
+  long long last_n = 0;
+};
+
+namespace lct {
+
+static __nv_bfloat16* act_buf(lct_cnn* c, int i) { return c->d_act + (size_t)i * c->act_elems; }
+static __nv_bfloat16* dz_buf(lct_cnn* c, int i) { return c->d_dz + (size_t)i * c->act_elems; }
+// input buffer of layer l (training keeps every activation; inference ping-pongs two)
+static int act_in(const lct_cnn* c, int l) { return c->train ? l : (l & 1); }
+
+static int act_map(CUtensorMap* m, const void* base, int cap, int H, int wp) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return LCT_ERR_UNSUPPORTED;
+  cuuint64_t dims[4] = {(cuuint64_t)kCnnC, (cuuint64_t)wp, (cuuint64_t)H, (cuuint64_t)cap};
+  cuuint64_t strides[3] = {(cuuint64_t)kCnnC * 2, (cuuint64_t)wp * kCnnC * 2,
+                           (cuuint64_t)H * wp * kCnnC * 2};
+  cuuint32_t box[4] = {(cuuint32_t)kCnnC, (cuuint32_t)kConvM, 1, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LCT_OK : LCT_ERR_UNSUPPORTED;
+}
+
+static int weight_map(CUtensorMap* m, const void* base, int rows) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return LCT_ERR_UNSUPPORTED;
+  cuuint64_t dims[2] = {(cuuint64_t)kCnnK, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kCnnK * 2};
+  cuuint32_t box[2] = {(cuuint32_t)kCnnC, (cuuint32_t)rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LCT_OK : LCT_ERR_UNSUPPORTED;
+}
+
+static bool conv_attr_done[64];
+
+static int conv_prepare(int dev) {
+  if (dev >= 0 && dev < 64 && conv_attr_done[dev]) return LCT_OK;
+  int st;
+  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<32, kEpiRelu>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             ConvCfg<32>::Smem))))
+    return st;
+  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<32, kEpiMask>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             ConvCfg<32>::Smem))))
+    return st;
+  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<16, kEpiResid>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             ConvCfg<16>::Smem))))
+    return st;
+  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<16, kEpiGate>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             ConvCfg<16>::Smem))))
+    return st;
+  if (dev >= 0 && dev < 64) conv_attr_done[dev] = true;
+  return LCT_OK;
+}
+
+template <int N, int EPI>
+static int launch_conv(const CUtensorMap& mx, const CUtensorMap& mw, const ConvArgs& a, int B,
+                       cudaStream_t s) {
+  const long long tiles = (long long)B * a.H * a.tiles_x;
+  if (tiles <= 0) return LCT_OK;
+  if (tiles > 0x7fffffffLL) return LCT_ERR_ARG;
+  conv_tc_kernel<N, EPI><<<(unsigned)tiles, kConvThreads, ConvCfg<N>::Smem, s>>>(mx, mw, a);
+  return launch_status();
+}
+
+static ConvArgs conv_args(const lct_cnn* c) {
+  ConvArgs a = {};
+  a.H = c->H;
+  a.W = c->W;
+  a.wp = c->wp;
+  a.tiles_x = (c->W + kConvM - 1) / kConvM;
+  a.status = device_status_ptr();
+  return a;
+}
+
+static int run_pack(lct_cnn* c, cudaStream_t s) {
+  cnn_pack_kernel<<<(kCnnLayers * kWSlot + 255) / 256, 256, 0, s>>>(c->d_p, c->d_wf, c->d_wb);
+  return launch_status();
+}
+
+static int run_prep(lct_cnn* c, const float* src, int vol_mode, int z0, int nz, int B,
+                    cudaStream_t s) {
+  const long long n = (long long)B * c->H * c->wp;
+  const float k_in = c->calib * c->in_scale;
+  cnn_prep_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, vol_mode, z0, nz, B, c->H,
+                                                             c->W, c->wp, k_in, act_buf(c, 0));
+  return launch_status();
+}
+
+// hidden layers 0..6 of the forward pass on B slices already in act_buf(0)
+static int run_hidden(lct_cnn* c, int B, cudaStream_t s) {
+  ConvArgs a = conv_args(c);
+  int st;
+  for (int l = 0; l < kCnnLayers - 1; ++l) {
+    a.bias = c->d_p + cnn_off(l) + cnn_cin(l) * cnn_cout(l) * 9;
+    a.out_act = act_buf(c, c->train ? l + 1 : ((l + 1) & 1));
+    if ((st = launch_conv<32, kEpiRelu>(c->m_act[act_in(c, l)], c->m_wf[l], a, B, s))) return st;
+  }
+  return LCT_OK;
+}
+
+static int last_bias_and_args(lct_cnn* c, ConvArgs& a) {
+  a = conv_args(c);
+  const int l = kCnnLayers - 1;
+  a.bias = c->d_p + cnn_off(l) + cnn_cin(l) * cnn_cout(l) * 9;
+  return LCT_OK;
+}
+
+static int cnn_forward_impl(lct_cnn* c, const float* d_in5, int B, cudaStream_t s) {
+  int st;
+  if ((st = run_prep(c, d_in5, 0, 0, 0, B, s))) return st;
+  if ((st = run_hidden(c, B, s))) return st;
+  ConvArgs a;
+  last_bias_and_args(c, a);
+  a.out_f = c->d_r;
+  return launch_conv<16, kEpiResid>(c->m_act[act_in(c, kCnnLayers - 1)], c->m_wf[kCnnLayers - 1],
+                                    a, B, s);
+}
+
+static int cnn_backward_impl(lct_cnn* c, const float* d_in5, const float* d_target, int B,
+                             cudaStream_t s) {
+  int st;
+  const long long n = (long long)B * c->H * c->W;
+  if ((st = cuda_status(cudaMemsetAsync(c->d_g, 0, sizeof(float) * kCnnParams, s)))) return st;
+  if ((st = cuda_status(cudaMemsetAsync(c->d_loss, 0, sizeof(double), s)))) return st;
+  cnn_loss_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      d_in5, c->d_r, d_target, B, c->H, c->W, c->wp, c->calib * c->in_scale, c->in_scale,
+      (float)(2.0 / (double)n), dz_buf(c, 2), c->d_loss);
+  if ((st = launch_status())) return st;
+  c->last_n = n;
+  const long long segs = (long long)B * c->H * ((c->W + kDwSeg - 1) / kDwSeg);
+  const int dw_grid = (int)(segs < (long long)c->sms * 4 ? segs : (long long)c->sms * 4);
+  ConvArgs a = conv_args(c);
+  int cur = 2;
+  for (int l = kCnnLayers - 1; l >= 0; --l) {
+    float* gw = c->d_g + cnn_off(l);
+    float* gb = gw + cnn_cin(l) * cnn_cout(l) * 9;
+    cnn_dw_kernel<<<dw_grid, kDwThreads, 0, s>>>(act_buf(c, l), dz_buf(c, cur), B, c->H, c->W,
+                                                 c->wp, cnn_cin(l), cnn_cout(l), gw, gb);
+    if ((st = launch_status())) return st;
+    if (l == 0) break;
+    const int nxt = cur == 2 ? 0 : (cur ^ 1);
+    a.out_act = dz_buf(c, nxt);
+    a.mask_act = act_buf(c, l);
+    if ((st = launch_conv<32, kEpiMask>(c->m_dz[cur], c->m_wb[l], a, B, s))) return st;
+    cur = nxt;
+  }
+  return LCT_OK;
+}
+
+static int cnn_adam_impl(lct_cnn* c, float lr, float b1, float b2, float eps, cudaStream_t s) {
+  ++c->adam_t;
+  const float c1 = (float)(1.0 / (1.0 - std::pow((double)b1, c->adam_t)));
+  const float c2 = (float)(1.0 / (1.0 - std::pow((double)b2, c->adam_t)));
+  cnn_adam_kernel<<<(kCnnParams + 255) / 256, 256, 0, s>>>(c->d_p, c->d_g, c->d_m, c->d_v,
+                                                          kCnnParams, lr, b1, b2, eps, c1, c2);
+  int st = launch_status();
+  return st ? st : run_pack(c, s);
+}
+
+// He-normal weights (std sqrt(2 / (9 cin)), the last layer x0.1 so training starts near the
+// identity), zero biases; splitmix64 + Box-Muller, so a seed gives the same network everywhere.
+static void init_params(std::vector<float>& p, uint64_t seed) {
+  uint64_t st = seed ^ 0x6c6374636e6eULL;
+  auto next = [&st]() {
+    uint64_t z = (st += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+  };
+  auto unif = [&]() { return ((double)(next() >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
+  p.assign(kCnnParams, 0.f);
+  for (int l = 0; l < kCnnLayers; ++l) {
+    const int nw = cnn_cin(l) * cnn_cout(l) * 9;
+    const double sd = std::sqrt(2.0 / (9.0 * cnn_cin(l))) * (l == kCnnLayers - 1 ? 0.1 : 1.0);
+    for (int i = 0; i < nw; ++i) {
+      const double u1 = unif(), u2 = unif();
+      p[cnn_off(l) + i] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) *
+                                  std::cos(2.0 * 3.141592653589793 * u2));
+    }
+  }
+}
+
+static void free_cnn(lct_cnn* c) {
+  if (!c) return;
+  cudaFree(c->d_p);
+  cudaFree(c->d_wf);
+  cudaFree(c->d_act);
+  cudaFree(c->d_dz);
+  cudaFree(c->d_r);
+  cudaFree(c->d_loss);
+  cudaFree(c->d_rej);
+  delete c;
+}
+
+}  // namespace lct
+
+LCT_API int lct_cnn_param_count(int64_t* n) {
+  if (!n) return LCT_ERR_ARG;
+  *n = kCnnParams;
+  return LCT_OK;
+}
+
+LCT_API int lct_cnn_create(int max_slices, int ny, int nx, int flags, uint64_t seed,
+                           lct_cnn** out) {
+  if (!out || max_slices <= 0 || ny <= 0 || nx <= 0) return LCT_ERR_ARG;
+  *out = nullptr;
+  if ((flags & ~LCT_CNN_TRAIN) != 0) return LCT_ERR_ARG;
+  const long long wp = (long long)nx + 2;
+  if (wp > (1LL << 31) / 2 || (long long)max_slices * ny * ((nx + kConvM - 1) / kConvM) > 0x7fffffffLL)
+    return LCT_ERR_ARG;
+  lct_cnn* c = new (std::nothrow) lct_cnn;
+  if (!c) return LCT_ERR_ALLOC;
+  c->cap = max_slices;
+  c->H = ny;
+  c->W = nx;
+  c->wp = (int)wp;
+  c->train = (flags & LCT_CNN_TRAIN) != 0;
+  c->n_act = c->train ? kCnnLayers : 2;
+  c->act_elems = (long long)max_slices * ny * wp * kCnnC;
+  int st = cuda_status(cudaGetDevice(&c->device));
+  if (!st) st = cuda_status(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device));
+  if (!st) st = conv_prepare(c->device);
+  if (!st) st = cuda_status(cudaMalloc(&c->d_p, sizeof(float) * 4 * kCnnParams));
+  if (!st) {
+    c->d_g = c->d_p + kCnnParams;
+    c->d_m = c->d_g + kCnnParams;
+    c->d_v = c->d_m + kCnnParams;
+    st = cuda_status(cudaMemset(c->d_p, 0, sizeof(float) * 4 * kCnnParams));
+  }
+  if (!st) st = cuda_status(cudaMalloc(&c->d_wf, sizeof(__nv_bfloat16) * 2 * kCnnLayers * kWSlot));
+  if (!st) c->d_wb = c->d_wf + kCnnLayers * kWSlot;
+  const size_t act_bytes = sizeof(__nv_bfloat16) * (size_t)c->act_elems;
+  if (!st) st = cuda_status(cudaMalloc(&c->d_act, act_bytes * c->n_act));
+  if (!st) st = cuda_status(cudaMemset(c->d_act, 0, act_bytes * c->n_act));
+  if (!st && c->train) {
+    st = cuda_status(cudaMalloc(&c->d_dz, act_bytes * 3));
+    if (!st) st = cuda_status(cudaMemset(c->d_dz, 0, act_bytes * 3));
+    if (!st) st = cuda_status(cudaMalloc(&c->d_r, sizeof(float) * (size_t)max_slices * ny * nx));
+  }
+  if (!st) st = cuda_status(cudaMalloc(&c->d_loss, sizeof(double)));
+  if (!st) st = cuda_status(cudaMalloc(&c->d_rej, sizeof(unsigned long long)));
+  for (int i = 0; i < c->n_act && !st; ++i) st = act_map(&c->m_act[i], act_buf(c, i), c->cap, c->H, c->wp);
+  for (int i = 0; i < 3 && !st && c->train; ++i)
+    st = act_map(&c->m_dz[i], dz_buf(c, i), c->cap, c->H, c->wp);
+  for (int l = 0; l < kCnnLayers && !st; ++l) {
+    st = weight_map(&c->m_wf[l], c->d_wf + (size_t)l * kWSlot, l == kCnnLayers - 1 ? 16 : 32);
+    if (!st) st = weight_map(&c->m_wb[l], c->d_wb + (size_t)l * kWSlot, 32);
+  }
+  if (!st) {
+    std::vector<float> p;
+    init_params(p, seed);
+    st = cuda_status(cudaMemcpy(c->d_p, p.data(), sizeof(float) * kCnnParams, cudaMemcpyHostToDevice));
+  }
+  if (!st) st = run_pack(c, nullptr);
+  if (!st) st = cuda_status(cudaDeviceSynchronize());
+  if (st) {
+    free_cnn(c);
+    return st;
+  }
+  *out = c;
+  return LCT_OK;
+}
+
+LCT_API int lct_cnn_set_params(lct_cnn* c, const float* params, int on_device) {
+  if (!c || !params) return LCT_ERR_ARG;
+  int st = cuda_status(cudaMemcpy(c->d_p, params, sizeof(float) * kCnnParams,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+  if (!st) st = cuda_status(cudaMemset(c->d_m, 0, sizeof(float) * 2 * kCnnParams));
+  c->adam_t = 0;
+  if (!st) st = run_pack(c, nullptr);
+  if (!st) st = cuda_status(cudaDeviceSynchronize());
+  return st;
+}
+
+LCT_API int lct_cnn_get_params(const lct_cnn* c, float* params, int on_device) {
+  if (!c || !params) return LCT_ERR_ARG;
+  return cuda_status(cudaMemcpy(params, c->d_p, sizeof(float) * kCnnParams,
+                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+}
+
+LCT_API int lct_cnn_get_grads(const lct_cnn* c, float* grads, int on_device) {
+  if (!c || !grads || !c->train) return LCT_ERR_ARG;
+  return cuda_status(cudaMemcpy(grads, c->d_g, sizeof(float) * kCnnParams,
+                                on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+}
+
+LCT_API int lct_cnn_set_scales(lct_cnn* c, float calib, float in_scale) {
+  if (!c || !(calib > 0.f) || !(in_scale > 0.f) || !std::isfinite(calib) || !std::isfinite(in_scale))
+    return LCT_ERR_ARG;
+  c->calib = calib;
+  c->in_scale = in_scale;
+  return LCT_OK;
+}
+
+LCT_API int lct_cnn_get_scales(const lct_cnn* c, float* calib, float* in_scale) {
+  if (!c || !calib || !in_scale) return LCT_ERR_ARG;
+  *calib = c->calib;
+  *in_scale = c->in_scale;
+  return LCT_OK;
+}
+
+LCT_API int lct_cnn_forward(lct_cnn* c, const float* d_in5, int n_slices, float* d_resid,
+                            lct_stream stream) {
+  if (!c || !d_in5 || n_slices <= 0 || n_slices > c->cap) return LCT_ERR_ARG;
+  if (!c->train) return LCT_ERR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cnn_forward_impl(c, d_in5, n_slices, s);
+  if (!st && d_resid)
+    st = cuda_status(cudaMemcpyAsync(d_resid, c->d_r, sizeof(float) * (size_t)n_slices * c->H * c->W,
+                                     cudaMemcpyDeviceToDevice, s));
+  return st;
+}
+
+LCT_API int lct_cnn_backward(lct_cnn* c, const float* d_in5, const float* d_target, int n_slices,
+                             lct_stream stream) {
+  if (!c || !d_in5 || !d_target || n_slices <= 0 || n_slices > c->cap) return LCT_ERR_ARG;
+  if (!c->train) return LCT_ERR_UNSUPPORTED;
+  return cnn_backward_impl(c, d_in5, d_target, n_slices, (cudaStream_t)stream);
+}
+
+LCT_API int lct_cnn_adam_step(lct_cnn* c, float lr, float beta1, float beta2, float eps,
+                              lct_stream stream) {
+  if (!c || !c->train || !(lr >= 0.f) || !(beta1 >= 0.f && beta1 < 1.f) ||
+      !(beta2 >= 0.f && beta2 < 1.f) || !(eps > 0.f))
+    return LCT_ERR_ARG;
+  return cnn_adam_impl(c, lr, beta1, beta2, eps, (cudaStream_t)stream);
+}
+
+LCT_API int lct_cnn_train_step(lct_cnn* c, const float* d_in5, const float* d_target,
+                               int n_slices, float lr, lct_stream stream) {
+  if (!c || !d_in5 || !d_target || n_slices <= 0 || n_slices > c->cap || !(lr >= 0.f))
+    return LCT_ERR_ARG;
+  if (!c->train) return LCT_ERR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cnn_forward_impl(c, d_in5, n_slices, s);
+  if (!st) st = cnn_backward_impl(c, d_in5, d_target, n_slices, s);
+  if (!st) st = cnn_adam_impl(c, lr, 0.9f, 0.999f, 1e-8f, s);
+  return st;
+}
+
+LCT_API int lct_cnn_last_loss(const lct_cnn* c, double* loss) {
+  if (!c || !loss || !c->train) return LCT_ERR_ARG;
+  if (c->last_n <= 0) return LCT_ERR_ARG;  // no backward pass yet
+  double sum = 0.0;
+  int st = cuda_status(cudaMemcpy(&sum, c->d_loss, sizeof(double), cudaMemcpyDeviceToHost));
+  if (!st) *loss = sum / (double)c->last_n;
+  return st;
+}
+
+LCT_API int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, int nz,
+                                 float bound, int64_t* n_rejected, lct_stream stream) {
+  if (!c || !d_vol || !d_out || nz <= 0 || d_vol == d_out || !(bound >= 0.f)) return LCT_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cuda_status(cudaMemsetAsync(c->d_rej, 0, sizeof(unsigned long long), s));
+  const long long plane = (long long)c->H * c->W;
+  for (int z0 = 0; z0 < nz && !st; z0 += c->cap) {
+    const int B = nz - z0 < c->cap ? nz - z0 : c->cap;
+    if ((st = run_prep(c, d_vol, 1, z0, nz, B, s))) break;
+    if ((st = run_hidden(c, B, s))) break;
+    ConvArgs a;
+    last_bias_and_args(c, a);
+    a.out_f = d_out + (size_t)z0 * plane;
+    a.xc = d_vol + (size_t)z0 * plane;
+    a.calib = c->calib;
+    a.inv_scale = 1.f / c->in_scale;
+    a.bound = bound;
+    a.n_reject = c->d_rej;
+    st = launch_conv<16, kEpiGate>(c->m_act[act_in(c, kCnnLayers - 1)], c->m_wf[kCnnLayers - 1],
+                                   a, B, s);
+  }
+  if (!st && n_rejected) {
+    unsigned long long v = 0;
+    st = cuda_status(cudaMemcpyAsync(&v, c->d_rej, sizeof(v), cudaMemcpyDeviceToHost, s));
+    if (!st) st = cuda_status(cudaStreamSynchronize(s));
+    if (!st) *n_rejected = (int64_t)v;
+  }
+  return st;
+}
+
+LCT_API void lct_cnn_destroy(lct_cnn* c) { free_cnn(c); }

@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static std::once_flag once;
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   std::call_once(once, [] {
@@ -255,7 +255,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // 2-D bf16 tensor [rows][cols] (cols contiguous), box {64, box_rows}, 128-byte swizzle
 static int make_map(CUtensorMap* map, const void* base, long long rows, int cols, int box_rows) {
-  auto fn = encode_fn();
+  auto fn = tensor_map_encoder();
   if (!fn) return LCT_ERR_UNSUPPORTED;
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)cols * 2};

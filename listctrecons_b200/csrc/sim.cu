@@ -111,9 +111,51 @@ __global__ void __launch_bounds__(128) sim_project_kernel(const double* __restri
   fan[((long long)blockIdx.z * nt + it) * ns + is] = (float)noisy_integral(p, i0, seed, idx);
 }
 
+// voxelised phantom: one thread per voxel, ss^3 sub-samples, ellipsoids in shared memory
+__global__ void __launch_bounds__(128) voxelise_kernel(const double* __restrict__ ell, int ne,
+                                                       int nx, int ny, double x0, double y0,
+                                                       double z0, double dx, double dy,
+                                                       double dz, int ss, float* __restrict__ out) {
+  __shared__ double s_e[kSimMaxEllipsoids * 16];
+  for (int i = threadIdx.x; i < ne * 16; i += blockDim.x) s_e[i] = ell[i];
+  __syncthreads();
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y, iz = blockIdx.z;
+  if (ix >= nx) return;
+  double acc = 0.0;
+  for (int sz = 0; sz < ss; ++sz)
+    for (int sy = 0; sy < ss; ++sy)
+      for (int sx = 0; sx < ss; ++sx) {
+        const double P[3] = {x0 + (ix + (sx + 0.5) / ss - 0.5) * dx,
+                             y0 + (iy + (sy + 0.5) / ss - 0.5) * dy,
+                             z0 + (iz + (sz + 0.5) / ss - 0.5) * dz};
+        for (int m = 0; m < ne; ++m) {
+          const double* e = s_e + 16 * m;
+          const double* R = e + 6;
+          const double p[3] = {P[0] - e[0], P[1] - e[1], P[2] - e[2]};
+          const double u0 = (R[0] * p[0] + R[3] * p[1] + R[6] * p[2]) / e[3];
+          const double u1 = (R[1] * p[0] + R[4] * p[1] + R[7] * p[2]) / e[4];
+          const double u2 = (R[2] * p[0] + R[5] * p[1] + R[8] * p[2]) / e[5];
+          if (u0 * u0 + u1 * u1 + u2 * u2 <= 1.0) acc += e[15];
+        }
+      }
+  out[((long long)iz * ny + iy) * nx + ix] = (float)(acc / ((double)ss * ss * ss));
+}
+
 }  // namespace lct
 
 using namespace lct;
+
+LCT_API int lct_voxelise(const double* d_ellipsoids, int n_ellipsoids, int nx, int ny, int nz,
+                         double x0, double y0, double z0, double dx, double dy, double dz, int ss,
+                         float* d_out, lct_stream stream) {
+  if (!d_ellipsoids || n_ellipsoids < 0 || n_ellipsoids > kSimMaxEllipsoids || !d_out) return LCT_ERR_ARG;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || ny > 65535 || nz > 65535 || ss <= 0 || ss > 16) return LCT_ERR_ARG;
+  dim3 grid((nx + 127) / 128, ny, nz);
+  voxelise_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(d_ellipsoids, n_ellipsoids, nx, ny, x0,
+                                                          y0, z0, dx, dy, dz, ss, d_out);
+  return launch_status();
+}
 
 LCT_API int lct_sim_project(const double* d_ellipsoids, int n_ellipsoids, int ns, int nt,
                             float ds, float dt, float ws, float wt, float dso,

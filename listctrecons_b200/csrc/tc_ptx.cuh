@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -9,6 +10,9 @@
 namespace lct {
 
 constexpr long long kTcWaitLimit = 1LL << 24;  // polls of an mbarrier before giving up
+
+// cuTensorMapEncodeTiled from the driver (resolved once; null when the driver lacks it)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // ---------------------------------------------------------------------------------------
 // PTX wrappers

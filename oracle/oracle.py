@@ -82,6 +82,10 @@ def lib() -> C.CDLL:
                                        C.c_uint64, P]),
             "orc_voxelise": (None, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                     C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, P]),
+            "orc_cnn_param_count": (C.c_int, []),
+            "orc_cnn_forward": (None, [P, P, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, P]),
+            "orc_cnn_loss_grad": (C.c_double, [P, P, P, C.c_int, C.c_int, C.c_int, C.c_float,
+                                               C.c_float, C.c_int, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(_lib, name)
@@ -235,6 +239,38 @@ def voxelise(ellipsoids, nx, ny, nz, x0, y0, z0, dx, dy, dz, ss=4):
     out = np.zeros((nz, ny, nx), dtype=np.float32)
     lib().orc_voxelise(e.ctypes.data, len(e), nx, ny, nz, x0, y0, z0, dx, dy, dz, ss, out.ctypes.data)
     return out
+
+
+# ------------------------------------------------------------------------------------------
+# learned correction (cnn_oracle.c)
+# ------------------------------------------------------------------------------------------
+CNN_CIN = (5, 32, 32, 32, 32, 32, 32, 32)
+CNN_COUT = (32, 32, 32, 32, 32, 32, 32, 1)
+
+
+def cnn_param_count() -> int:
+    return lib().orc_cnn_param_count()
+
+
+def cnn_forward(params, in5, k_in: float, bf16: bool = True) -> np.ndarray:
+    """Residual r [B][H][W] (network units) for 5-slice inputs in5 [B][5][H][W]."""
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    x = _f32(in5)
+    B, _, H, W = x.shape
+    r = np.zeros((B, H, W), dtype=np.float64)
+    lib().orc_cnn_forward(p.ctypes.data, x.ctypes.data, B, H, W, float(k_in), int(bf16), r.ctypes.data)
+    return r
+
+
+def cnn_loss_grad(params, in5, target, k_in: float, s: float, bf16: bool = True):
+    """(loss, gradient) of mean((k_in x_c + r - s t)^2) with respect to the parameters."""
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    x, t = _f32(in5), _f32(target)
+    B, _, H, W = x.shape
+    g = np.zeros_like(p)
+    loss = lib().orc_cnn_loss_grad(p.ctypes.data, x.ctypes.data, t.ctypes.data, B, H, W,
+                                   float(k_in), float(s), int(bf16), g.ctypes.data)
+    return loss, g
 
 
 def rel_l2(a, b) -> float:
