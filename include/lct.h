@@ -357,7 +357,18 @@ int lct_cnn_last_loss(const lct_cnn* c, double* loss);
    value; when given, the call synchronises the stream. */
 int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, int nz, float bound,
                          int64_t* n_rejected, lct_stream stream);
+/* rejected-voxel count of the last infer_volume (synchronous; call after its stream finished) */
+int lct_cnn_last_rejected(const lct_cnn* c, int64_t* n);
+int lct_cnn_get_shape(const lct_cnn* c, int* max_slices, int* ny, int* nx);
 void lct_cnn_destroy(lct_cnn* c);
+
+/* Fused learned correction in lct_recon_run (c = NULL turns it off; c is not owned and must
+   outlive its use; its ny, nx must match the plan's image).  The run then backprojects into an
+   internal plain volume and writes the gated corrected volume to `image`.  learned_info: ms of
+   the correction in the last run (inside the backprojection -> download span of
+   lct_recon_last_times) and its rejected-voxel count; either pointer may be NULL. */
+int lct_recon_set_learned(lct_recon* r, lct_cnn* c, float bound);
+int lct_recon_learned_info(const lct_recon* r, float* ms, int64_t* rejected);
 
 /* ---------------------------------------------------------------------------------------
  * Diagnostics

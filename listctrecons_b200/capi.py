@@ -174,7 +174,11 @@ SIGNATURES: dict[str, tuple] = {
     "lct_cnn_train_step": (I32, [P, P, P, I32, F32, P]),
     "lct_cnn_last_loss": (I32, [P, P]),
     "lct_cnn_infer_volume": (I32, [P, P, P, I32, F32, P, P]),
+    "lct_cnn_last_rejected": (I32, [P, P]),
+    "lct_cnn_get_shape": (I32, [P, P, P, P]),
     "lct_cnn_destroy": (None, [P]),
+    "lct_recon_set_learned": (I32, [P, P, F32]),
+    "lct_recon_learned_info": (I32, [P, P, P]),
 }
 
 _lib: C.CDLL | None = None

@@ -818,4 +818,20 @@ LCT_API int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, i
   return st;
 }
 
+LCT_API int lct_cnn_get_shape(const lct_cnn* c, int* max_slices, int* ny, int* nx) {
+  if (!c || !max_slices || !ny || !nx) return LCT_ERR_ARG;
+  *max_slices = c->cap;
+  *ny = c->H;
+  *nx = c->W;
+  return LCT_OK;
+}
+
+LCT_API int lct_cnn_last_rejected(const lct_cnn* c, int64_t* n) {
+  if (!c || !n) return LCT_ERR_ARG;
+  unsigned long long v = 0;
+  int st = cuda_status(cudaMemcpy(&v, c->d_rej, sizeof(v), cudaMemcpyDeviceToHost));
+  if (!st) *n = (int64_t)v;
+  return st;
+}
+
 LCT_API void lct_cnn_destroy(lct_cnn* c) { free_cnn(c); }

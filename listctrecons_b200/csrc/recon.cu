@@ -38,7 +38,10 @@ static void free_recon(lct_recon* r) {
   cudaFree(r->d_img);
   cudaFree(r->d_quad);
   cudaFree(r->d_tc);
+  cudaFree(r->d_plain);
   for (auto& e : r->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : r->ev_cnn)
     if (e) cudaEventDestroy(e);
   delete r;
 }
@@ -483,7 +486,8 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     d_fan = r->d_fan;
   }
   if ((st = cuda_status(cudaEventRecord(r->ev[1], s)))) return st;
-  float* d_img = image_on_device ? image : r->d_img;
+  float* d_out = image_on_device ? image : r->d_img;
+  float* d_img = r->cnn ? r->d_plain : d_out;  // backprojection target
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
 
   if (r->o.mode == LCT_MODE_BLOCK) {
@@ -500,6 +504,16 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     if ((st = recon_stage_bp(r, d_img, s))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
   }
+  if (r->cnn) {  // fused learned correction: plain volume -> gated corrected volume
+    if ((st = cuda_status(cudaEventRecord(r->ev_cnn[0], s)))) return st;
+    if ((st = lct_cnn_infer_volume(r->cnn, d_img, d_out, nb * kBlockSlices, r->cnn_bound, nullptr,
+                                   stream)))
+      return st;
+    if ((st = cuda_status(cudaEventRecord(r->ev_cnn[1], s)))) return st;
+    int ms = 0, ny = 0, nx = 0;
+    lct_cnn_get_shape(r->cnn, &ms, &ny, &nx);
+    r->launches += 1 + 9 * ((nb * kBlockSlices + ms - 1) / ms);  // memset + (prep + 8 convs) per pass
+  }
 
   if (!image_on_device) {
     if ((st = cuda_status(cudaMemcpyAsync(image, r->d_img, sizeof(float) * nb * slab,
@@ -512,6 +526,39 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     float ms = 0.f;
     cudaEventElapsedTime(&ms, r->ev[i], r->ev[i + 1]);
     r->times[i] = ms;
+  }
+  r->cnn_ms = 0.f;
+  if (r->cnn) cudaEventElapsedTime(&r->cnn_ms, r->ev_cnn[0], r->ev_cnn[1]);
+  return LCT_OK;
+}
+
+LCT_API int lct_recon_set_learned(lct_recon* r, lct_cnn* c, float bound) {
+  if (!r || !(bound >= 0.f)) return LCT_ERR_ARG;
+  if (!c) {
+    r->cnn = nullptr;
+    return LCT_OK;
+  }
+  int ms = 0, ny = 0, nx = 0;
+  int st = lct_cnn_get_shape(c, &ms, &ny, &nx);
+  if (st) return st;
+  if (ny != r->info.ig.ny || nx != r->info.ig.nx) return LCT_ERR_ARG;
+  const size_t img_elems =
+      (size_t)r->info.n_blocks_run * kBlockSlices * r->info.ig.nx * r->info.ig.ny;
+  if (!r->d_plain && (st = cuda_status(cudaMalloc(&r->d_plain, sizeof(float) * img_elems))))
+    return st;
+  for (auto& e : r->ev_cnn)
+    if (!e && (st = cuda_status(cudaEventCreate(&e)))) return st;
+  r->cnn = c;
+  r->cnn_bound = bound;
+  return LCT_OK;
+}
+
+LCT_API int lct_recon_learned_info(const lct_recon* r, float* ms, int64_t* rejected) {
+  if (!r) return LCT_ERR_ARG;
+  if (ms) *ms = r->cnn ? r->cnn_ms : 0.f;
+  if (rejected) {
+    *rejected = 0;
+    if (r->cnn) return lct_cnn_last_rejected(r->cnn, rejected);
   }
   return LCT_OK;
 }

@@ -23,6 +23,11 @@ struct lct_recon {
   bool quads = false;        // full windows: the quad-layout pairs kernel applies
   cudaEvent_t ev[6] = {};
   float times[5] = {};
+  lct_cnn* cnn = nullptr;    // learned correction after backprojection (not owned)
+  float cnn_bound = 0.f;
+  float* d_plain = nullptr;  // plain FDK volume when the learned correction runs
+  cudaEvent_t ev_cnn[2] = {};
+  float cnn_ms = 0.f;
   int device = 0;
   long long voxel_updates = 0;
   int launches = 0;

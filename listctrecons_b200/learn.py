@@ -27,7 +27,7 @@ from .scan import MU_WATER, Phantom, ScanGeometry, simulate_gpu
 N_PARAMS = 57249
 CIN = (5, 32, 32, 32, 32, 32, 32, 32)
 COUT = (32, 32, 32, 32, 32, 32, 32, 1)
-DEFAULT_BOUND = 0.5 * MU_WATER  # 1/mm: largest accepted |corrected - plain|
+DEFAULT_BOUND = 2.0 * MU_WATER  # 1/mm: largest accepted |corrected - plain| (densest single ellipsoid)
 
 
 def _torch():

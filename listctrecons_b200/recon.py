@@ -129,6 +129,25 @@ class Reconstruction:
         capi.check(self._lib.lct_recon_stats_get(self._h, C.byref(st)))
         return st
 
+    def set_learned(self, cnn, bound: float | None = None) -> None:
+        """Fuse the learned correction (learn.CNN, inference workspace of this image's ny x nx)
+        after backprojection; None turns it off.  run() then returns the corrected volume."""
+        if cnn is None:
+            capi.check(self._lib.lct_recon_set_learned(self._h, None, 0.0), "lct_recon_set_learned")
+            self._cnn = None
+            return
+        from .learn import DEFAULT_BOUND
+
+        b = DEFAULT_BOUND if bound is None else bound
+        capi.check(self._lib.lct_recon_set_learned(self._h, cnn._h, float(b)),
+                   "lct_recon_set_learned")
+        self._cnn = cnn  # keep it alive while fused
+
+    def learned_info(self) -> dict:
+        ms, rej = C.c_float(), C.c_int64()
+        capi.check(self._lib.lct_recon_learned_info(self._h, C.byref(ms), C.byref(rej)))
+        return {"ms": ms.value, "rejected": rej.value}
+
     def autotune(self) -> tuple[int, int]:
         nz, mb = C.c_int(), C.c_int()
         capi.check(self._lib.lct_recon_autotune(self._h, C.byref(nz), C.byref(mb)))

@@ -142,26 +142,64 @@ def test_voxelise_matches_oracle(cuda):
 
 def test_training_gain_over_plain_fdk(cuda):
     """Train on seeded pairs, evaluate on held-out seeds: the corrected volume is closer to the
-    phantom than calibrated plain FDK."""
-    from listctrecons_b200.learn import (CNN, PairGenerator, evaluate, fit_calibration,
-                                         pair_spec, train)
+    phantom than calibrated plain FDK, with the acceptance gate at its default bound and without
+    it."""
+    from listctrecons_b200.learn import (CNN, DEFAULT_BOUND, PairGenerator, evaluate,
+                                         fit_calibration, pair_spec, train)
     from listctrecons_b200.scan import MU_WATER
 
     spec = pair_spec(ns=256, nt=16, ds=1.0, npt=480, pitch=1.5, nx=128, dx=1.5, dz=1.5, nz=32,
                      n_ellipsoids=20)
     spec.semi = (4.0, 50.0)
     gen = PairGenerator(spec)
-    train_pairs = [tuple(x.clone() for x in gen.pair(1000 + i)) for i in range(12)]
-    test_pairs = [tuple(x.clone() for x in gen.pair(9000 + i)) for i in range(3)]
+    train_pairs = [tuple(x.clone() for x in gen.pair(1000 + i)) for i in range(24)]
+    test_pairs = [tuple(x.clone() for x in gen.pair(9000 + i)) for i in range(4)]
     _, H, W = gen.shape
-    cnn = CNN(8, H, W, train=True, seed=1)
+    cnn = CNN(16, H, W, train=True, seed=1)
     cnn.set_scales(fit_calibration(train_pairs), 1.0 / MU_WATER)
-    before = evaluate(cnn, test_pairs)
-    train(cnn, train_pairs, steps=400, batch=8, lr=1e-3, log_every=100)
-    inf = CNN(16, H, W, train=False)
+    before = evaluate(cnn, test_pairs, bound=1e30)
+    train(cnn, train_pairs, steps=1500, batch=16, lr=2e-3, log_every=500)
+    inf = CNN(32, H, W, train=False)
     inf.copy_from(cnn)
-    after = evaluate(inf, test_pairs)
-    print("before training:", before)
-    print("after training: ", after)
-    assert after["plain_rel_l2"] < 0.5  # the voxel grid lines up with the FDK volume
-    assert after["corrected_rel_l2"] < 0.95 * after["plain_rel_l2"], after
+    gated = evaluate(inf, test_pairs, bound=DEFAULT_BOUND)
+    free = evaluate(inf, test_pairs, bound=1e30)
+    print("before training (no gate):", before)
+    print(f"after training, gate {DEFAULT_BOUND / MU_WATER:g} mu_water:", gated)
+    print("after training, no gate:", free)
+    assert gated["plain_rel_l2"] < 0.5  # the voxel grid lines up with the FDK volume
+    assert gated["corrected_rel_l2"] < 0.9 * gated["plain_rel_l2"], gated
+    assert free["corrected_rel_l2"] < 0.75 * free["plain_rel_l2"], free
+    assert gated["rejected_fraction"] < 0.02, gated
+
+
+def test_fused_recon_equals_separate(cuda):
+    """lct_recon_run with the correction attached == plain run, then infer_volume (bit-exact),
+    in scan mode from device and from host buffers."""
+    import torch
+
+    from listctrecons_b200 import capi
+    from listctrecons_b200.learn import CNN
+    from listctrecons_b200.recon import Plan, Reconstruction
+    from listctrecons_b200.scan import Phantom, ScanGeometry, simulate_gpu
+
+    geo = ScanGeometry(ns=160, nt=16, ds=1.0, dt=1.0, npt=240, pitch=1.0, nx=48, ny=48, dx=1.5,
+                       dz=1.0).with_blocks(2)
+    plan = Plan(geo)
+    ph = Phantom.random(6, seed=3, fov_radius=30.0, z_lo=plan.blocks[0].block_start,
+                        z_hi=plan.blocks[1].block_end, semi=(4.0, 14.0))
+    fan = simulate_gpu(geo, ph, i0=1e5, seed=4)
+    rec = Reconstruction(plan, mode=capi.MODE_SCAN)
+    plain = rec.run(fan).clone()
+    cnn = CNN(16, 48, 48, train=False, seed=7)
+    cnn.set_scales(0.5, 50.0)
+    sep, rej_sep = cnn.infer_volume(plain, bound=0.04)
+    rec.set_learned(cnn, bound=0.04)
+    fused = rec.run(fan)
+    info = rec.learned_info()
+    assert torch.equal(fused, sep)
+    assert info["rejected"] == rej_sep and info["ms"] > 0
+    host = torch.empty(fused.shape, dtype=torch.float32).pin_memory()
+    rec.run(fan.cpu().pin_memory(), image=host)
+    assert torch.equal(host, sep.cpu())
+    rec.set_learned(None)
+    assert torch.equal(rec.run(fan), plain)
