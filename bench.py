@@ -16,6 +16,13 @@ A step = one full reconstruction of that volume.
 Multi-GPU (torchrun): weak scaling, rank r reconstructs blocks [8r, 8r+8) of one longer scan,
 no data-path collective; step time = max over ranks.
 
+Every run also times the same reconstruction with the learned correction fused after the
+backprojection (`mixed_learned`: lct_recon_set_learned, weights trained on the learned
+configuration, listctrecons_b200/weights/cnn_cfg4.npz).  `--workload cfg4` is that learned
+configuration itself (736 x 64 @ 0.6 mm, pitch 1.5, 256 x 256 x 64 @ 1 mm, 40 ellipsoids):
+plain vs corrected error against the phantom on held-out seeded scans, fused timing, and the
+training throughput of the project's own kernels.
+
 `--impl reference` times the reference's formulas on the host CPU (the CPU oracle's FP32
 restatement, every core): the reference has no CPU implementation of the path, so this is a
 port; each step is a bounded sample extrapolated to the whole volume.
@@ -43,6 +50,15 @@ METRIC = "FDK voxel-GUPS & s/volume at relL2<=1e-4 vs FP64 oracle: plain vs mixe
 UNIT = "voxel-GUPS"
 FALLBACK_HBM_GBS = 6650.0
 FALLBACK_BF16_TFLOPS = 1590.0
+WEIGHTS = ROOT / "listctrecons_b200" / "weights" / "cnn_cfg4.npz"
+CNN_FLOP_PER_VOXEL = 114048  # 2*9*(5*32 + 6*32*32 + 32*1), forward
+# algorithmic HBM bytes per voxel of one inference pass: prep reads 4 B and writes a 64 B
+# activation, 7 layers read 64 B and write 64 B, the last reads 64 B + the plain voxel and writes
+# the corrected one
+CNN_BYTES_PER_VOXEL = 4 + 64 + 7 * 128 + 64 + 4 + 4
+CFG4_LABEL = ("learned configuration: helical FDK 736x64@0.6mm, 1152 views/rot, pitch 1.5, "
+              "256x256x64@1mm, 40 ellipsoids, I0=1e5, Ram-Lak, then the 2.5D residual CNN "
+              "(8 conv3x3 x 32 ch, BF16) fused after backprojection")
 
 WORKLOADS = {
     "cfg2": dict(
@@ -411,6 +427,192 @@ def run_reference(args, rank, world):
     return 0
 
 
+def timed(fn, steps, stream):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = []
+    e0.record(stream)
+    for _ in range(steps):
+        out.append(fn())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, out
+
+
+def learned_cnn(ny, nx, max_slices=32):
+    """Inference network for the fused leg: the trained weights when present, else He-init
+    (the timing does not depend on the weight values)."""
+    from listctrecons_b200.learn import CNN, cnn_from_weights, load_weights
+    from listctrecons_b200.scan import MU_WATER
+
+    if WEIGHTS.exists():
+        meta = load_weights(WEIGHTS)["meta"]
+        return (cnn_from_weights(WEIGHTS, max_slices, ny, nx),
+                f"trained: {meta.get('train_pairs')} pairs, {meta.get('steps')} steps "
+                f"({WEIGHTS.relative_to(ROOT)})")
+    c = CNN(max_slices, ny, nx, train=False)
+    c.set_scales(0.5, 1.0 / MU_WATER)
+    return c, "He-init (no weights file)"
+
+
+def learned_leg(args, rec, fan, h_fan, f0, maxr, barrier, stream, bound):
+    """The same reconstruction with the learned correction fused after backprojection (own
+    output buffers: the plain volume of the main leg stays untouched)."""
+    import torch
+
+    ig = rec.plan.info.ig
+    img = torch.empty(rec.image_shape, dtype=torch.float32, device=fan.device)
+    h_img = torch.empty(rec.image_shape, dtype=torch.float32, pin_memory=True)
+    nvox = rec.image_shape[0] * ig.ny * ig.nx
+    cnn, src = learned_cnn(ig.ny, ig.nx)
+    rec.set_learned(cnn, bound)
+    for _ in range(max(1, args.warmup)):
+        rec.run(fan, img, fan_view0=f0)
+    barrier()
+    torch.cuda.synchronize()
+    ms, infos = timed(lambda: (rec.run(fan, img, fan_view0=f0), rec.learned_info())[1],
+                      args.steps, stream)
+    ms = maxr(ms)
+    launches = rec.stats().launches * args.steps
+    rec.run(h_fan, h_img, fan_view0=f0)
+    barrier()
+    torch.cuda.synchronize()
+    e2e_ms, _ = timed(lambda: rec.run(h_fan, h_img, fan_view0=f0), args.steps, stream)
+    e2e_ms = maxr(e2e_ms)
+    launches += rec.stats().launches * args.steps
+    rec.set_learned(None)
+    cnn_ms = statistics.mean(i["ms"] for i in infos)
+    peak_t = measured_peak_tflops()
+    peak_b, _, _ = measured_peaks()
+    upd = rec.stats().voxel_updates
+    tfl = nvox * CNN_FLOP_PER_VOXEL / (cnn_ms / 1e3) / 1e12
+    gbs = nvox * CNN_BYTES_PER_VOXEL / (cnn_ms / 1e3) / 1e9
+    return {
+        "value": upd / (ms / 1e3) / 1e9, "unit": UNIT, "s_per_volume": ms / 1e3,
+        "e2e": {"value": upd / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "s_per_volume": e2e_ms / 1e3},
+        "cnn_ms": cnn_ms, "cnn_share": cnn_ms / ms,
+        "cnn_roofline": {"bound": "hbm", "achieved": gbs, "peak": peak_b, "unit": "GB/s",
+                         "frac": gbs / peak_b, "algorithmic_bytes_per_voxel": CNN_BYTES_PER_VOXEL,
+                         "tflops": tfl, "tensor_frac": tfl / peak_t[0]},
+        "rejected_fraction": statistics.mean(i["rejected"] for i in infos) / nvox,
+        "bound_per_mm": bound, "weights": src,
+    }, launches
+
+
+def measured_peak_tflops():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("bf16_tflops", FALLBACK_BF16_TFLOPS), "measured"
+    return FALLBACK_BF16_TFLOPS, "fallback"
+
+
+def run_learned(args, rank, world, dist):
+    """The learned configuration (config 4): held-out accuracy, plain vs fused timing, training
+    throughput.  Weak scaling over ranks: each rank reconstructs its own held-out scans."""
+    import torch
+
+    from listctrecons_b200.learn import (CNN, DEFAULT_BOUND, PairGenerator, evaluate,
+                                         load_weights, mixed_opts, pair_spec, stack5)
+    from listctrecons_b200.scan import MU_WATER, simulate_gpu
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    spec = pair_spec()
+    gen = PairGenerator(spec, **mixed_opts())
+    rec, plan = gen.rec, gen.plan
+    _, H, W = gen.shape
+    cnn, src = learned_cnn(H, W, max_slices=64)
+    seeds = [900000 + 1000 * rank + i for i in range(args.eval_pairs)]
+    test = [tuple(x.clone() for x in gen.pair(s)) for s in seeds]
+    bound = args.bound * MU_WATER if args.bound is not None else DEFAULT_BOUND
+    acc = {"plain_vs_phantom": None, "gated": {}, "ungated": None}
+    for b in (1.0, 2.0, 5.0, 10.0):
+        e = evaluate(cnn, test, bound=b * MU_WATER)
+        acc["gated"][f"{b:g}_mu_water"] = {k: e[k] for k in ("corrected_rel_l2", "corrected_rmse",
+                                                            "rejected_fraction")}
+        acc["plain_vs_phantom"] = {k: e[k] for k in ("plain_rel_l2", "plain_rmse")}
+    e = evaluate(cnn, test, bound=1e30)
+    acc["ungated"] = {k: e[k] for k in ("corrected_rel_l2", "corrected_rmse")}
+    acc["calib"] = e["calib"]
+    acc["eval"] = f"{len(test)} held-out seeded scans (seeds {seeds[0]}..{seeds[-1]})"
+    del test
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def maxr(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ph = gen.phantom(seeds[0])
+    f0 = rec.fan_first
+    fan = simulate_gpu(spec.geo, ph, i0=spec.i0, seed=seeds[0], v0=f0, v1=f0 + rec.fan_count).clone()
+    img = torch.empty(gen.shape, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        rec.run(fan, img, fan_view0=f0)
+    barrier()
+    torch.cuda.synchronize()
+    plain_ms, _ = timed(lambda: rec.run(fan, img, fan_view0=f0), args.steps, stream)
+    plain_ms = maxr(plain_ms)
+    launches = rec.stats().launches * args.steps
+    h_fan = torch.empty(fan.shape, dtype=torch.float32, pin_memory=True)
+    h_fan.copy_(fan)
+    props = torch.cuda.get_device_properties(dev)
+    uuid = str(getattr(props, "uuid", "")) if hasattr(props, "uuid") else ""
+    clocks = ClockSampler(("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or "0"))
+    time.sleep(0.3)
+    leg, n = learned_leg(args, rec, fan, h_fan, f0, maxr, barrier, stream, bound)
+    launches += n
+    # training throughput of the project's kernels (forward + backward + Adam), timing only
+    tr = CNN(16, H, W, train=True)
+    if WEIGHTS.exists():
+        tr.set_params(load_weights(WEIGHTS)["params"])
+    tr.set_scales(*cnn.scales())
+    fdk = rec.run(fan, fan_view0=f0)
+    tgt = gen.target(ph)
+    z = np.arange(16) * (fdk.shape[0] // 16)
+    x, t = stack5(fdk, z).contiguous(), tgt[torch.as_tensor(z, device=dev)].contiguous()
+    tr.train_step(x, t, 0.0)
+    torch.cuda.synchronize()
+    t_ms, _ = timed(lambda: tr.train_step(x, t, 0.0), 20, stream)
+    clk = clocks.stop()
+    if rank != 0:
+        return 0
+    upd = rec.stats().voxel_updates * world
+    pix = 16 * H * W
+    line = {
+        "metric": METRIC, "value": upd / (leg["s_per_volume"]) / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": leg["s_per_volume"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+        "data": "synthetic (seeded 40-ellipsoid phantoms, analytic helical scans + Poisson I0=1e5, "
+                "simulated on the GPU; training and evaluation seeds disjoint)",
+        "config": {"workload": CFG4_LABEL, "volume": list(gen.shape),
+                   "recon": "scan mode, BF16x6 filter, exact interpolation",
+                   "l2": "fan %.2f GB > L2" % (rec.fan_count * spec.geo.nt * spec.geo.ns * 4 / 1e9),
+                   "parallelism": f"independent scans x{world}"},
+        "s_per_volume": leg["s_per_volume"],
+        "plain": {"value": upd / (plain_ms / 1e3) / 1e9, "unit": UNIT, "s_per_volume": plain_ms / 1e3},
+        "mixed_learned": leg,
+        "e2e": {"value": leg["e2e"]["value"] * world, "unit": UNIT,
+                "s_per_volume": leg["e2e"]["s_per_volume"],
+                "h2d_bytes_per_step": rec.stats().h2d_bytes, "d2h_bytes_per_step": rec.stats().d2h_bytes},
+        "accuracy_vs_phantom": acc,
+        "training": {"ms_per_step": t_ms, "slices_per_step": 16,
+                     "tflops": pix * 3 * CNN_FLOP_PER_VOXEL / (t_ms / 1e3) / 1e12,
+                     "note": "forward + backward (tcgen05 data gradients, SIMT weight gradients) + Adam"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -489,6 +691,16 @@ def run_ours(args, rank, world, dist):
     barrier()
     e2e_ms = maxr(e2.elapsed_time(e3) / args.steps)
     launches += rec.stats().launches * args.steps
+    learned = None
+    if not args.no_learned:
+        from listctrecons_b200.learn import DEFAULT_BOUND
+        from listctrecons_b200.scan import MU_WATER
+
+        bound = args.bound * MU_WATER if args.bound is not None else DEFAULT_BOUND
+        learned, n = learned_leg(args, rec, fan, h_fan, f0, maxr, barrier, stream, bound)
+        learned["note"] = ("timing of the fused correction on this volume; its accuracy against "
+                           "the phantom is measured on the learned configuration (--workload cfg4)")
+        launches += n
     clk = clocks.stop()
 
     updates_all = st.voxel_updates * world
@@ -528,6 +740,7 @@ def run_ours(args, rank, world, dist):
         "e2e": {"value": e2e, "unit": UNIT, "s_per_volume": e2e_ms / 1e3,
                 "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
         "gpu_launches": launches,
+        "mixed_learned": learned,
         "roofline": {"kernel": "bp_quad_kernel", "bound": "hbm", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
@@ -562,7 +775,7 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3", "cfg4"])
     ap.add_argument("--mode", default="scan", choices=["scan", "block"])
     ap.add_argument("--filter", default="bf16x6", choices=["fp32", "bf16x3", "bf16x6"],
                     help="bf16x6: tensor-core Toeplitz GEMM with 3-way bf16 splits (meets the "
@@ -576,6 +789,10 @@ def main() -> int:
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the fused learned-correction leg")
+    ap.add_argument("--bound", type=float, default=None,
+                    help="acceptance-gate bound in units of mu_water (default 10)")
+    ap.add_argument("--eval-pairs", type=int, default=4, help="held-out scans (cfg4)")
     ap.add_argument("--plain-gpu", action="store_true",
                     help="also time the reference program itself on the same scan (slow)")
     args = ap.parse_args()
@@ -602,6 +819,8 @@ def main() -> int:
     try:
         if args.workload == "cfg3":
             return run_batch(args, rank, world, dist)
+        if args.workload == "cfg4":
+            return run_learned(args, rank, world, dist)
         return run_ours(args, rank, world, dist)
     finally:
         if dist is not None:

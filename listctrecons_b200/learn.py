@@ -27,7 +27,11 @@ from .scan import MU_WATER, Phantom, ScanGeometry, simulate_gpu
 N_PARAMS = 57249
 CIN = (5, 32, 32, 32, 32, 32, 32, 32)
 COUT = (32, 32, 32, 32, 32, 32, 32, 1)
-DEFAULT_BOUND = 2.0 * MU_WATER  # 1/mm: largest accepted |corrected - plain| (densest single ellipsoid)
+# 1/mm: largest accepted |corrected - plain|.  On the learned configuration plain FDK is off by
+# several mu_water where photons starve (40 overlapping ellipsoids, I0 = 1e5) and at pitch 1.5;
+# a 2 mu_water gate rejects 14% of the voxels and keeps little of the correction, 10 mu_water
+# rejects 0.35% (the benchmark reports the sweep).
+DEFAULT_BOUND = 10.0 * MU_WATER
 
 
 def _torch():
@@ -165,6 +169,13 @@ class PairSpec:
     ss: int = 4                # voxelisation sub-samples per axis
 
 
+# recon options of the training pairs and of the learned configuration: the mixed-precision path
+# (tensor-core BF16x6 Toeplitz filter, FP64-geometry exact interpolation), Ram-Lak taps
+def mixed_opts() -> dict:
+    return dict(filter_mode=capi.FILTER_BF16X6, interp=capi.INTERP_EXACT,
+                filter_kind=capi.FILTER_RAMLAK)
+
+
 def pair_spec(ns=736, nt=64, ds=0.6, npt=1152, pitch=1.5, nx=256, dx=1.0, dz=1.0, nz=64,
               n_ellipsoids=40, i0=1e5) -> PairSpec:
     """A training geometry: scan length = the planner minimum for nz slices (nz / 32 blocks).
@@ -286,3 +297,92 @@ def evaluate(cnn: CNN, pairs, bound: float = DEFAULT_BOUND) -> dict:
             "plain_rel_l2": (plain_se / ref_sq) ** 0.5, "corrected_rel_l2": (corr_se / ref_sq) ** 0.5,
             "rejected_fraction": rejected / voxels, "bound": bound, "calib": calib,
             "volumes": len(pairs)}
+
+
+# ------------------------------------------------------------------------------------------
+# weights files and the training command
+# ------------------------------------------------------------------------------------------
+def save_weights(path, cnn: CNN, meta: dict) -> None:
+    import json
+    from pathlib import Path
+
+    calib, in_scale = cnn.scales()
+    Path(path).parent.mkdir(parents=True, exist_ok=True)
+    np.savez(path, params=cnn.params(), calib=np.float32(calib), in_scale=np.float32(in_scale),
+             meta=np.array(json.dumps(meta)))
+
+
+def load_weights(path) -> dict:
+    import json
+
+    with np.load(path) as z:
+        return {"params": z["params"].astype(np.float32), "calib": float(z["calib"]),
+                "in_scale": float(z["in_scale"]), "meta": json.loads(str(z["meta"]))}
+
+
+def cnn_from_weights(path, max_slices: int, ny: int, nx: int, train: bool = False) -> CNN:
+    w = load_weights(path)
+    c = CNN(max_slices, ny, nx, train=train)
+    c.set_params(w["params"])
+    c.set_scales(w["calib"], w["in_scale"])
+    return c
+
+
+def _train_main(argv=None) -> int:
+    """python -m listctrecons_b200.learn train --out FILE [...]: seeded training pairs of the
+    736 x 64 @ 0.6 mm, pitch 1.5, 256 x 256 x 64 @ 1 mm configuration (40 ellipsoids), Adam on
+    the GPU, evaluation on held-out seeds; writes the weights and a JSON summary."""
+    import argparse
+    import json
+    import time
+
+    torch = _torch()
+    ap = argparse.ArgumentParser(prog="python -m listctrecons_b200.learn train")
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--pairs", type=int, default=256)
+    ap.add_argument("--test-pairs", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    spec = pair_spec()
+    gen = PairGenerator(spec, **mixed_opts())
+    t0 = time.perf_counter()
+    pairs = [tuple(x.clone() for x in gen.pair(100000 * (a.seed + 1) + i)) for i in range(a.pairs)]
+    test = [tuple(x.clone() for x in gen.pair(900000 + 1000 * a.seed + i))
+            for i in range(a.test_pairs)]
+    torch.cuda.synchronize()
+    t_pairs = time.perf_counter() - t0
+    _, H, W = gen.shape
+    cnn = CNN(a.batch, H, W, train=True, seed=a.seed)
+    cnn.set_scales(fit_calibration(pairs), 1.0 / MU_WATER)
+    t0 = time.perf_counter()
+    train(cnn, pairs, steps=a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log_every=500)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    inf = CNN(32, H, W, train=False)
+    inf.copy_from(cnn)
+    meta = {
+        "geometry": "736x64@0.6mm, 1152 views/rot, pitch 1.5, 256x256x64@1mm, 40 ellipsoids, I0=1e5",
+        "recon": "scan mode, Ram-Lak, BF16x6 tensor-core filter, exact interpolation",
+        "train_pairs": a.pairs, "train_seeds": f"{100000 * (a.seed + 1)}+i",
+        "test_pairs": a.test_pairs, "test_seeds": f"{900000 + 1000 * a.seed}+i",
+        "steps": a.steps, "batch_slices": a.batch, "lr": a.lr, "seed": a.seed,
+        "pair_generation_s": t_pairs, "training_s": t_train,
+        "eval_gated": evaluate(inf, test, bound=DEFAULT_BOUND),
+        "eval_ungated": evaluate(inf, test, bound=1e30),
+    }
+    save_weights(a.out, cnn, meta)
+    print(json.dumps(meta), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+
+    if len(sys.argv) > 1 and sys.argv[1] == "train":
+        sys.exit(_train_main(sys.argv[2:]))
+    print("usage: python -m listctrecons_b200.learn train --out FILE [--pairs N] [--steps N]")
+    sys.exit(2)

@@ -117,6 +117,10 @@ class Reconstruction:
         torch = _torch()
         if image is None:
             image = torch.empty(self.image_shape, dtype=torch.float32, device="cuda")
+        g = self.plan.info.ctg
+        _check_views(fan, self.fan_first, self.fan_count, int(fan_view0), g.ns * g.nt)
+        if int(np.prod(image.shape)) < int(np.prod(self.image_shape)):
+            raise ValueError(f"image smaller than {self.image_shape}")
         f_dev, f_ptr = _ptr(fan)
         i_dev, i_ptr = _ptr(image)
         s = stream if stream is not None else _stream()
@@ -191,6 +195,14 @@ class Batch:
         n = len(self.plans)
         if images is None:
             images = [torch.empty(sh, dtype=torch.float32, device="cuda") for sh in self.image_shapes]
+        for i, (f, p) in enumerate(zip(fans, self.plans)):
+            first, count = self.fan_ranges[i]
+            g = p.info.ctg
+            _check_views(f, first, count, int((fan_view0 or [0] * n)[i]), g.ns * g.nt,
+                         what=f"fan {i}")
+        for i, sh in zip(images, self.image_shapes):
+            if int(np.prod(i.shape)) < int(np.prod(sh)):
+                raise ValueError(f"image smaller than {sh}")
         fp = [_ptr(f) for f in fans]
         ip = [_ptr(i) for i in images]
         if len({d for d, _ in fp}) != 1 or len({d for d, _ in ip}) != 1:
@@ -218,6 +230,18 @@ class Batch:
         if h:
             self._lib.lct_batch_destroy(h)
             self._h = None
+
+
+def _check_views(x, first: int, count: int, view0: int, plane: int, what: str = "fan") -> None:
+    """The buffer must hold views [first, first + count) counted from view0 (the C ABI takes a
+    bare pointer and cannot check it)."""
+    if first < view0:
+        raise ValueError(f"{what} starts at view {view0} but the run needs view {first}")
+    need = (first + count - view0) * plane
+    have = int(np.prod(x.shape)) if hasattr(x, "shape") else None
+    if have is not None and have < need:
+        raise ValueError(f"{what} holds {have // plane} views from view {view0}; the run reads "
+                         f"views {first}..{first + count - 1}")
 
 
 def _ptr(x):
