@@ -9,12 +9,13 @@
 // pixel; one zero pad column on each side, pixel x at column x+1; channels beyond a layer's
 // width are zero).  Weights are packed per layer as bf16 [N][9 taps x 32 channels].
 //
-// Convolution = implicit GEMM on tcgen05: a CTA computes 128 consecutive pixels of one image
-// row x N output channels (N = 32, or 16 for the 1-channel last layer) over K = 9 taps x 32
-// channels.  Per tap, one 4-D TMA box {32 ch, 128 px, 1 row, 1 slice} with 64-byte swizzle
-// lands in a 4-stage ring (rows above/below the image come back as TMA's zero fill); the
-// packed weights (9 x N x 64 bytes) sit in shared memory; two M128 x N x K16 MMAs per tap
-// accumulate in TMEM.  Fused epilogues: bias + ReLU -> bf16 (forward), ReLU mask of the
+// Convolution = implicit GEMM on tcgen05 in a persistent, warp-specialised kernel: a tile is
+// 8 px x 16 rows (M 128) x N output channels (N = 32, or 16 for the 1-channel last layer) over
+// K = 9 taps x 32 channels.  Per tile, three 4-D TMA boxes {32 ch, 8 px, 18 rows, 1 slice} with
+// 64-byte swizzle (one per column offset; rows outside the image come back as TMA's zero fill)
+// serve all nine taps, each row offset being a whole swizzle atom; the packed weights
+// (9 x N x 64 bytes) are loaded once per CTA; two M128 x N x K16 MMAs per tap accumulate in one
+// of two TMEM buffers.  Fused epilogues: bias + ReLU -> bf16 (forward), ReLU mask of the
 // previous activation -> bf16 delta (backward data), FP32 residual (training), and the
 // acceptance gate writing the corrected volume (inference).
 // Weight gradients: SIMT FP32 outer products over row segments staged in shared memory.
@@ -31,8 +32,11 @@ namespace lct {
 
 constexpr int kCnnLayers = 8, kCnnC = 32, kCnnTaps = 9, kCnnK = kCnnTaps * kCnnC;  // K = 288
 constexpr int kCnnParams = 57249;     // sum over layers of cin*cout*9 + cout
-constexpr int kConvM = 128, kConvStages = 4, kConvThreads = 128;
 constexpr int kWSlot = kCnnC * kCnnK;  // packed weights of one layer, elements
+// output tile 8 px x 16 rows = the M 128 of one MMA; M row m = row * 8 + px
+constexpr int kConvTW = 8, kConvTH = 16, kConvM = kConvTW * kConvTH;
+constexpr int kConvStages = 6;    // A boxes in flight (3 per tile)
+constexpr int kConvThreads = 192; // warp 0 TMA, warp 1 MMA + TMEM, warps 2-5 epilogue
 
 LCT_HD constexpr int cnn_cin(int l) { return l == 0 ? 5 : 32; }
 LCT_HD constexpr int cnn_cout(int l) { return l == kCnnLayers - 1 ? 1 : 32; }
@@ -41,7 +45,8 @@ LCT_HD constexpr int cnn_off(int l) { return l == 0 ? 0 : 1472 + (l - 1) * 9248;
 enum ConvEpi : int { kEpiRelu = 0, kEpiMask = 1, kEpiResid = 2, kEpiGate = 3 };
 
 struct ConvArgs {
-  int H, W, wp, tiles_x;
+  int H, W, wp, tiles_x, tiles_y;
+  long long n_tiles;
   const float* bias;               // [N] (forward epilogues)
   __nv_bfloat16* out_act;          // Relu / Mask: [B][H][wp][32]
   const __nv_bfloat16* mask_act;   // Mask: activation whose sign gates the delta
@@ -54,11 +59,13 @@ struct ConvArgs {
 
 template <int N>
 struct ConvCfg {
-  static constexpr uint32_t TileA = kConvM * kCnnC * 2;  // 8 KB per tap
+  // one A box: 32 channels x 8 px x 18 rows (the tile's rows and one halo row on each side)
+  static constexpr uint32_t BoxA = kConvTW * (kConvTH + 2) * kCnnC * 2;  // 9216 B
+  static constexpr uint32_t RowA = kConvTW * kCnnC * 2;                  // 512 B = one atom
   static constexpr uint32_t TapB = N * kCnnC * 2;        // 2 KB (N=32) or 1 KB (N=16)
   static constexpr uint32_t BBytes = kCnnTaps * TapB;
-  static constexpr uint32_t Smem = 1024 + kConvStages * TileA + BBytes + 128;
-  static constexpr uint32_t TmemCols = 32;
+  static constexpr uint32_t Smem = 1024 + kConvStages * BoxA + BBytes + 256;
+  static constexpr uint32_t TmemCols = 64;  // two 32-column accumulators
   static constexpr uint32_t Idesc = (1u << 4) | (1u << 7) | (1u << 10) |
                                     ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kConvM >> 4) << 24);
 };
@@ -70,8 +77,27 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
 __device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
 
+__device__ __forceinline__ void conv_tile(const ConvArgs& a, long long t, int& x0, int& y0,
+                                          int& b) {
+  const long long per = (long long)a.tiles_x * a.tiles_y;
+  b = (int)(t / per);
+  const int r = (int)(t % per);
+  y0 = (r / a.tiles_x) * kConvTH;
+  x0 = (r % a.tiles_x) * kConvTW;
+}
+
+__device__ __forceinline__ bool conv_aborted(int* flag) {
+  return *reinterpret_cast<volatile int*>(flag) != 0;
+}
+
+// Persistent implicit-GEMM 3x3 convolution: CTA c takes tiles c, c + grid, ...  Per tile, three
+// A boxes (one per column offset dx) feed nine taps: tap (dy, dx) reads box dx from row dy,
+// i.e. at +dy * 512 bytes -- a whole 64-byte-swizzle atom, so every operand start stays on the
+// swizzle pattern.  Two TMEM accumulators let the epilogue of one tile overlap the MMAs of the
+// next.  Every wait is bounded; on a timeout the CTA drains its copies and MMAs, raises the
+// device status word and leaves its remaining tiles unwritten.
 template <int N, int EPI>
-__global__ void __launch_bounds__(kConvThreads, 4)
+__global__ void __launch_bounds__(kConvThreads)
     conv_tc_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
                    const ConvArgs a) {
   using Cfg = ConvCfg<N>;
@@ -79,20 +105,19 @@ __global__ void __launch_bounds__(kConvThreads, 4)
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   uint8_t* sa = smem;
-  uint8_t* sb = smem + kConvStages * Cfg::TileA;
+  uint8_t* sb = smem + kConvStages * Cfg::BoxA;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sb + Cfg::BBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kConvStages + 2);
+  // full[S] empty[S] wbar acc_full[2] acc_empty[2] mma_done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kConvStages + 6);
   __shared__ int s_abort;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int t = blockIdx.x;
-  const int xt = t % a.tiles_x, q = t / a.tiles_x;
-  const int y = q % a.H, b = q / a.H;
-  const int x0 = xt * kConvM;
   const uint32_t full0 = smem_u32(&bars[0]);
   const uint32_t empty0 = smem_u32(&bars[kConvStages]);
   const uint32_t wbar = smem_u32(&bars[2 * kConvStages]);
-  const uint32_t accum = smem_u32(&bars[2 * kConvStages + 1]);
+  const uint32_t accf0 = smem_u32(&bars[2 * kConvStages + 1]);
+  const uint32_t acce0 = smem_u32(&bars[2 * kConvStages + 3]);
+  const uint32_t mdone = smem_u32(&bars[2 * kConvStages + 5]);
 
   if (threadIdx.x == 0) {
     s_abort = 0;
@@ -101,10 +126,14 @@ __global__ void __launch_bounds__(kConvThreads, 4)
       mbar_init(empty0 + 8 * s, 1);
     }
     mbar_init(wbar, 1);
-    mbar_init(accum, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(accf0 + 8 * i, 1);
+      mbar_init(acce0 + 8 * i, 4);  // one arrival per epilogue warp
+    }
+    mbar_init(mdone, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
                  "r"(Cfg::TmemCols)
@@ -116,121 +145,168 @@ __global__ void __launch_bounds__(kConvThreads, 4)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0 && lane == 0) {
-    // producer: the layer's packed weights once, then one A box per tap
-    mbar_expect_tx(wbar, Cfg::BBytes);
-    for (int k = 0; k < kCnnTaps; ++k)
-      tma_load_2d(smem_u32(sb + k * Cfg::TapB), &mw, k * kCnnC, 0, wbar);
-    int issued = 0;
-    for (int k = 0; k < kCnnTaps; ++k) {
-      const int s = k % kConvStages;
-      if (k >= kConvStages && !mbar_wait(empty0 + 8 * s, ((k / kConvStages) - 1) & 1)) {
-        atomicExch(&s_abort, 1);
-        break;
+  if (warp == 0) {
+    if (lane == 0) {
+      // producer: the layer's packed weights once, then three A boxes per tile
+      mbar_expect_tx(wbar, Cfg::BBytes);
+      for (int k = 0; k < kCnnTaps; ++k)
+        tma_load_2d(smem_u32(sb + k * Cfg::TapB), &mw, k * kCnnC, 0, wbar);
+      long long kg = 0;
+      bool stop = false;
+      for (long long t = blockIdx.x; t < a.n_tiles && !stop; t += gridDim.x) {
+        int x0, y0, b;
+        conv_tile(a, t, x0, y0, b);
+        for (int l = 0; l < 3; ++l, ++kg) {
+          const int s = (int)(kg % kConvStages);
+          if (kg >= kConvStages &&
+              !mbar_wait(empty0 + 8 * s, (uint32_t)(((kg / kConvStages) - 1) & 1))) {
+            atomicExch(&s_abort, 1);
+            stop = true;
+            break;
+          }
+          if (conv_aborted(&s_abort)) {
+            stop = true;
+            break;
+          }
+          mbar_expect_tx(full0 + 8 * s, Cfg::BoxA);
+          // pixel x of the tile, column offset dx = l - 1, sits at padded column x + l
+          tma_load_4d(smem_u32(sa + s * Cfg::BoxA), &mx, 0, x0 + l, y0 - 1, b, full0 + 8 * s);
+        }
       }
-      if (atomicAdd(&s_abort, 0)) break;
-      const int dy = k / 3 - 1, dx = k % 3 - 1;
-      mbar_expect_tx(full0 + 8 * s, Cfg::TileA);
-      // pixel x of the tile reads column x + 1 + dx of the padded rows
-      tma_load_4d(smem_u32(sa + s * Cfg::TileA), &mx, 0, x0 + 1 + dx, y + dy, b, full0 + 8 * s);
-      issued = k + 1;
+      if (conv_aborted(&s_abort)) {  // let copies in flight land before the CTA exits
+        mbar_wait(wbar, 0);
+        for (long long k = (kg > kConvStages ? kg - kConvStages : 0); k < kg; ++k)
+          mbar_wait(full0 + 8 * (int)(k % kConvStages), (uint32_t)((k / kConvStages) & 1));
+      }
     }
-    if (atomicAdd(&s_abort, 0)) {  // let copies in flight land before the CTA exits
-      mbar_wait(wbar, 0);
-      for (int k = (issued > kConvStages ? issued - kConvStages : 0); k < issued; ++k)
-        mbar_wait(full0 + 8 * (k % kConvStages), (k / kConvStages) & 1);
-    }
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer
-    if (!mbar_wait(wbar, 0)) {
-      atomicExch(&s_abort, 1);
-    } else {
-      for (int k = 0; k < kCnnTaps; ++k) {
-        const int s = k % kConvStages;
-        if (!mbar_wait(full0 + 8 * s, (k / kConvStages) & 1)) {
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer
+      bool ok = mbar_wait(wbar, 0);
+      if (!ok) atomicExch(&s_abort, 1);
+      long long kg = 0;
+      int it = 0;
+      for (long long t = blockIdx.x; t < a.n_tiles && ok; t += gridDim.x, ++it) {
+        const int buf = it & 1;
+        if (it >= 2 && !mbar_wait(acce0 + 8 * buf, (uint32_t)(((it >> 1) - 1) & 1))) {
           atomicExch(&s_abort, 1);
           break;
         }
+        if (conv_aborted(&s_abort)) break;
         tc_fence_after();
-        const uint64_t da = desc_sw64(smem_u32(sa + s * Cfg::TileA));
-        const uint64_t db = desc_sw64(smem_u32(sb + k * Cfg::TapB));
-        umma_bf16(tmem, da, db, Cfg::Idesc, k ? 1u : 0u);
-        umma_bf16(tmem, da + 2, db + 2, Cfg::Idesc, 1u);  // +32 bytes: channels 16..31
-        umma_commit(empty0 + 8 * s);
+        const uint32_t d = tmem + (uint32_t)(buf * 32);
+        for (int l = 0; l < 3 && ok; ++l, ++kg) {
+          const int s = (int)(kg % kConvStages);
+          if (!mbar_wait(full0 + 8 * s, (uint32_t)((kg / kConvStages) & 1))) {
+            atomicExch(&s_abort, 1);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t base = smem_u32(sa + s * Cfg::BoxA);
+#pragma unroll
+          for (int dy = 0; dy < 3; ++dy) {
+            const uint64_t da = desc_sw64(base + dy * Cfg::RowA);
+            const uint64_t db = desc_sw64(smem_u32(sb + (dy * 3 + l) * Cfg::TapB));
+            umma_bf16(d, da, db, Cfg::Idesc, (l | dy) ? 1u : 0u);
+            umma_bf16(d, da + 2, db + 2, Cfg::Idesc, 1u);  // +32 bytes: channels 16..31
+          }
+          umma_commit(empty0 + 8 * s);
+        }
+        if (!ok) break;
+        umma_commit(accf0 + 8 * buf);
       }
+      umma_commit(mdone);  // every MMA issued above has finished once this arrives
+      if (!mbar_wait(mdone, 0)) atomicExch(&s_abort, 1);
     }
-    umma_commit(accum);
-  }
-  __syncwarp();
-
-  const bool done = mbar_wait(accum, 0);
-  __syncthreads();
-  tc_fence_after();
-  const bool ok = done && !*reinterpret_cast<volatile int*>(&s_abort);
-  if (!ok) {
-    if (threadIdx.x == 0 && a.status) atomicExch(a.status, kDevWaitTimeout);
   } else {
-    const int i = warp * 32 + lane;
-    const int x = x0 + i;
-    const bool in = x < a.W;
-    const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16);
-    if constexpr (N == 32) {
-      uint32_t r[32];
-      tmem_ld32(ta, r);
-      if (in) {
-        const long long pix = ((long long)b * a.H + y) * a.wp + x + 1;
-        uint4* dst = reinterpret_cast<uint4*>(a.out_act + pix * kCnnC);
-        if constexpr (EPI == kEpiRelu) {
-#pragma unroll
-          for (int g = 0; g < 4; ++g) {
-            float v[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j)
-              v[j] = fmaxf(__uint_as_float(r[8 * g + j]) + __ldg(a.bias + 8 * g + j), 0.f);
-            dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
-                                pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
-          }
-        } else {
-          const uint4* msk = reinterpret_cast<const uint4*>(a.mask_act + pix * kCnnC);
-#pragma unroll
-          for (int g = 0; g < 4; ++g) {
-            const uint4 mv = msk[g];
-            const uint32_t mwd[4] = {mv.x, mv.y, mv.z, mv.w};
-            float v[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              const int16_t bits = (int16_t)((mwd[j >> 1] >> (16 * (j & 1))) & 0xFFFFu);
-              v[j] = bits > 0 ? __uint_as_float(r[8 * g + j]) : 0.f;
-            }
-            dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
-                                pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
-          }
-        }
+    // epilogue: warp w reads TMEM lanes 32 * (w % 4) ... + 31
+    const int qd = warp & 3;
+    const int m = qd * 32 + lane;
+    const int yy = m / kConvTW, px = m % kConvTW;
+    int it = 0;
+    for (long long t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int buf = it & 1;
+      // warp-uniform decision: the TMEM load below is .sync.aligned
+      const bool got = __all_sync(0xFFFFFFFFu, mbar_wait(accf0 + 8 * buf, (uint32_t)((it >> 1) & 1)));
+      if (!got) {
+        if (lane == 0) atomicExch(&s_abort, 1);
+        break;
       }
-    } else {
-      uint32_t r[16];
-      tmem_ld16(ta, r);
-      const long long o = ((long long)b * a.H + y) * a.W + x;
-      const float rr = __uint_as_float(r[0]) + __ldg(a.bias);
-      if constexpr (EPI == kEpiResid) {
-        if (in) a.out_f[o] = rr;
-      } else {
-        bool rej = false;
+      if (__any_sync(0xFFFFFFFFu, conv_aborted(&s_abort))) break;
+      tc_fence_after();
+      int x0, y0, b;
+      conv_tile(a, t, x0, y0, b);
+      const int x = x0 + px, y = y0 + yy;
+      const bool in = x < a.W && y < a.H;
+      const uint32_t ta = tmem + (uint32_t)(buf * 32) + ((uint32_t)(qd * 32) << 16);
+      if constexpr (N == 32) {
+        uint32_t r[32];
+        tmem_ld32(ta, r);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce0 + 8 * buf);
         if (in) {
-          const float plain = a.calib * a.xc[o];
-          const float d = rr * a.inv_scale;
-          const bool keep = fabsf(d) <= a.bound;  // NaN fails the test: plain is kept
-          a.out_f[o] = keep ? plain + d : plain;
-          rej = !keep;
+          const long long pix = ((long long)b * a.H + y) * a.wp + x + 1;
+          uint4* dst = reinterpret_cast<uint4*>(a.out_act + pix * kCnnC);
+          if constexpr (EPI == kEpiRelu) {
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+              float v[8];
+#pragma unroll
+              for (int j = 0; j < 8; ++j)
+                v[j] = fmaxf(__uint_as_float(r[8 * g + j]) + __ldg(a.bias + 8 * g + j), 0.f);
+              dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
+                                  pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+            }
+          } else {
+            const uint4* msk = reinterpret_cast<const uint4*>(a.mask_act + pix * kCnnC);
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+              const uint4 mv = msk[g];
+              const uint32_t mwd[4] = {mv.x, mv.y, mv.z, mv.w};
+              float v[8];
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                const int16_t bits = (int16_t)((mwd[j >> 1] >> (16 * (j & 1))) & 0xFFFFu);
+                v[j] = bits > 0 ? __uint_as_float(r[8 * g + j]) : 0.f;
+              }
+              dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
+                                  pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
+            }
+          }
         }
-        const unsigned m = __ballot_sync(0xFFFFFFFFu, rej);
-        if (lane == 0 && m && a.n_reject) atomicAdd(a.n_reject, (unsigned long long)__popc(m));
+      } else {
+        uint32_t r[16];
+        tmem_ld16(ta, r);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce0 + 8 * buf);
+        const long long o = ((long long)b * a.H + y) * a.W + x;
+        const float rr = __uint_as_float(r[0]) + __ldg(a.bias);
+        if constexpr (EPI == kEpiResid) {
+          if (in) a.out_f[o] = rr;
+        } else {
+          bool rej = false;
+          if (in) {
+            const float plain = a.calib * a.xc[o];
+            const float dlt = rr * a.inv_scale;
+            const bool keep = fabsf(dlt) <= a.bound;  // NaN fails the test: plain is kept
+            a.out_f[o] = keep ? plain + dlt : plain;
+            rej = !keep;
+          }
+          const unsigned msk = __ballot_sync(0xFFFFFFFFu, rej);
+          if (lane == 0 && msk && a.n_reject)
+            atomicAdd(a.n_reject, (unsigned long long)__popc(msk));
+        }
       }
     }
   }
+
   tc_fence_before();
   __syncthreads();
-  if (warp == 0)
+  if (threadIdx.x == 0 && conv_aborted(&s_abort) && a.status) atomicExch(a.status, kDevWaitTimeout);
+  if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(Cfg::TmemCols)
                  : "memory");
@@ -447,7 +523,7 @@ static int act_map(CUtensorMap* m, const void* base, int cap, int H, int wp) {
   cuuint64_t dims[4] = {(cuuint64_t)kCnnC, (cuuint64_t)wp, (cuuint64_t)H, (cuuint64_t)cap};
   cuuint64_t strides[3] = {(cuuint64_t)kCnnC * 2, (cuuint64_t)wp * kCnnC * 2,
                            (cuuint64_t)H * wp * kCnnC * 2};
-  cuuint32_t box[4] = {(cuuint32_t)kCnnC, (cuuint32_t)kConvM, 1, 1};
+  cuuint32_t box[4] = {(cuuint32_t)kCnnC, (cuuint32_t)kConvTW, (cuuint32_t)(kConvTH + 2), 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides,
                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
@@ -468,38 +544,44 @@ static int weight_map(CUtensorMap* m, const void* base, int rows) {
   return r == CUDA_SUCCESS ? LCT_OK : LCT_ERR_UNSUPPORTED;
 }
 
+// per device: dynamic shared memory set, and resident CTAs per SM of each variant
 static bool conv_attr_done[64];
+static int conv_occ[64][2];
+
+template <int N, int EPI>
+static int conv_attr(int* occ) {
+  int st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<N, EPI>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            ConvCfg<N>::Smem));
+  if (!st)
+    st = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, conv_tc_kernel<N, EPI>,
+                                                                   kConvThreads, ConvCfg<N>::Smem));
+  if (!st && *occ < 1) st = LCT_ERR_UNSUPPORTED;
+  return st;
+}
 
 static int conv_prepare(int dev) {
-  if (dev >= 0 && dev < 64 && conv_attr_done[dev]) return LCT_OK;
-  int st;
-  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<32, kEpiRelu>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             ConvCfg<32>::Smem))))
-    return st;
-  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<32, kEpiMask>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             ConvCfg<32>::Smem))))
-    return st;
-  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<16, kEpiResid>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             ConvCfg<16>::Smem))))
-    return st;
-  if ((st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<16, kEpiGate>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             ConvCfg<16>::Smem))))
-    return st;
-  if (dev >= 0 && dev < 64) conv_attr_done[dev] = true;
+  if (dev < 0 || dev >= 64) return LCT_ERR_UNSUPPORTED;
+  if (conv_attr_done[dev]) return LCT_OK;
+  int st, o[4];
+  if ((st = conv_attr<32, kEpiRelu>(&o[0]))) return st;
+  if ((st = conv_attr<32, kEpiMask>(&o[1]))) return st;
+  if ((st = conv_attr<16, kEpiResid>(&o[2]))) return st;
+  if ((st = conv_attr<16, kEpiGate>(&o[3]))) return st;
+  conv_occ[dev][0] = o[0] < o[1] ? o[0] : o[1];
+  conv_occ[dev][1] = o[2] < o[3] ? o[2] : o[3];
+  conv_attr_done[dev] = true;
   return LCT_OK;
 }
 
 template <int N, int EPI>
-static int launch_conv(const CUtensorMap& mx, const CUtensorMap& mw, const ConvArgs& a, int B,
-                       cudaStream_t s) {
-  const long long tiles = (long long)B * a.H * a.tiles_x;
-  if (tiles <= 0) return LCT_OK;
-  if (tiles > 0x7fffffffLL) return LCT_ERR_ARG;
-  conv_tc_kernel<N, EPI><<<(unsigned)tiles, kConvThreads, ConvCfg<N>::Smem, s>>>(mx, mw, a);
+static int launch_conv(const CUtensorMap& mx, const CUtensorMap& mw, ConvArgs a, int B, int dev,
+                       int sms, cudaStream_t s) {
+  a.n_tiles = (long long)B * a.tiles_x * a.tiles_y;
+  if (a.n_tiles <= 0) return LCT_OK;
+  const long long resident = (long long)sms * conv_occ[dev][N == 32 ? 0 : 1];
+  const unsigned grid = (unsigned)(a.n_tiles < resident ? a.n_tiles : resident);
+  conv_tc_kernel<N, EPI><<<grid, kConvThreads, ConvCfg<N>::Smem, s>>>(mx, mw, a);
   return launch_status();
 }
 
@@ -508,7 +590,8 @@ static ConvArgs conv_args(const lct_cnn* c) {
   a.H = c->H;
   a.W = c->W;
   a.wp = c->wp;
-  a.tiles_x = (c->W + kConvM - 1) / kConvM;
+  a.tiles_x = (c->W + kConvTW - 1) / kConvTW;
+  a.tiles_y = (c->H + kConvTH - 1) / kConvTH;
   a.status = device_status_ptr();
   return a;
 }
@@ -534,7 +617,9 @@ static int run_hidden(lct_cnn* c, int B, cudaStream_t s) {
   for (int l = 0; l < kCnnLayers - 1; ++l) {
     a.bias = c->d_p + cnn_off(l) + cnn_cin(l) * cnn_cout(l) * 9;
     a.out_act = act_buf(c, c->train ? l + 1 : ((l + 1) & 1));
-    if ((st = launch_conv<32, kEpiRelu>(c->m_act[act_in(c, l)], c->m_wf[l], a, B, s))) return st;
+    if ((st = launch_conv<32, kEpiRelu>(c->m_act[act_in(c, l)], c->m_wf[l], a, B, c->device,
+                                        c->sms, s)))
+      return st;
   }
   return LCT_OK;
 }
@@ -554,7 +639,7 @@ static int cnn_forward_impl(lct_cnn* c, const float* d_in5, int B, cudaStream_t 
   last_bias_and_args(c, a);
   a.out_f = c->d_r;
   return launch_conv<16, kEpiResid>(c->m_act[act_in(c, kCnnLayers - 1)], c->m_wf[kCnnLayers - 1],
-                                    a, B, s);
+                                    a, B, c->device, c->sms, s);
 }
 
 static int cnn_backward_impl(lct_cnn* c, const float* d_in5, const float* d_target, int B,
@@ -582,7 +667,8 @@ static int cnn_backward_impl(lct_cnn* c, const float* d_in5, const float* d_targ
     const int nxt = cur == 2 ? 0 : (cur ^ 1);
     a.out_act = dz_buf(c, nxt);
     a.mask_act = act_buf(c, l);
-    if ((st = launch_conv<32, kEpiMask>(c->m_dz[cur], c->m_wb[l], a, B, s))) return st;
+    if ((st = launch_conv<32, kEpiMask>(c->m_dz[cur], c->m_wb[l], a, B, c->device, c->sms, s)))
+      return st;
     cur = nxt;
   }
   return LCT_OK;
@@ -647,8 +733,7 @@ LCT_API int lct_cnn_create(int max_slices, int ny, int nx, int flags, uint64_t s
   *out = nullptr;
   if ((flags & ~LCT_CNN_TRAIN) != 0) return LCT_ERR_ARG;
   const long long wp = (long long)nx + 2;
-  if (wp > (1LL << 31) / 2 || (long long)max_slices * ny * ((nx + kConvM - 1) / kConvM) > 0x7fffffffLL)
-    return LCT_ERR_ARG;
+  if (wp > (1LL << 30) || ny > (1 << 30)) return LCT_ERR_ARG;
   lct_cnn* c = new (std::nothrow) lct_cnn;
   if (!c) return LCT_ERR_ALLOC;
   c->cap = max_slices;
@@ -807,7 +892,7 @@ LCT_API int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, i
     a.bound = bound;
     a.n_reject = c->d_rej;
     st = launch_conv<16, kEpiGate>(c->m_act[act_in(c, kCnnLayers - 1)], c->m_wf[kCnnLayers - 1],
-                                   a, B, s);
+                                   a, B, c->device, c->sms, s);
   }
   if (!st && n_rejected) {
     unsigned long long v = 0;

@@ -26,7 +26,7 @@ def _random_params(seed):
     return p
 
 
-@pytest.mark.parametrize("shape", [(2, 12, 40), (2, 9, 136), (1, 4, 256)])
+@pytest.mark.parametrize("shape", [(2, 12, 40), (2, 9, 136), (1, 4, 256), (1, 37, 45)])
 def test_forward_matches_oracle(cuda, shape):
     import torch
 
