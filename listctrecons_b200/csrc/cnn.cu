@@ -97,7 +97,7 @@ __device__ __forceinline__ bool conv_aborted(int* flag) {
 // next.  Every wait is bounded; on a timeout the CTA drains its copies and MMAs, raises the
 // device status word and leaves its remaining tiles unwritten.
 template <int N, int EPI>
-__global__ void __launch_bounds__(kConvThreads)
+__global__ void __launch_bounds__(kConvThreads, 3)
     conv_tc_kernel(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mw,
                    const ConvArgs a) {
   using Cfg = ConvCfg<N>;
@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(kConvThreads)
   // full[S] empty[S] wbar acc_full[2] acc_empty[2] mma_done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kConvStages + 6);
   __shared__ int s_abort;
+  __shared__ float s_bias[32];  // the layer's biases, read by every tile's epilogue
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t full0 = smem_u32(&bars[0]);
@@ -119,6 +120,8 @@ __global__ void __launch_bounds__(kConvThreads)
   const uint32_t acce0 = smem_u32(&bars[2 * kConvStages + 3]);
   const uint32_t mdone = smem_u32(&bars[2 * kConvStages + 5]);
 
+  if (threadIdx.x < 32)
+    s_bias[threadIdx.x] = (EPI != kEpiMask && threadIdx.x < N) ? a.bias[threadIdx.x] : 0.f;
   if (threadIdx.x == 0) {
     s_abort = 0;
     for (int s = 0; s < kConvStages; ++s) {
@@ -224,6 +227,7 @@ __global__ void __launch_bounds__(kConvThreads)
     const int qd = warp & 3;
     const int m = qd * 32 + lane;
     const int yy = m / kConvTW, px = m % kConvTW;
+    const float* bias = s_bias;
     int it = 0;
     for (long long t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
       const int buf = it & 1;
@@ -255,7 +259,7 @@ __global__ void __launch_bounds__(kConvThreads)
               float v[8];
 #pragma unroll
               for (int j = 0; j < 8; ++j)
-                v[j] = fmaxf(__uint_as_float(r[8 * g + j]) + __ldg(a.bias + 8 * g + j), 0.f);
+                v[j] = fmaxf(__uint_as_float(r[8 * g + j]) + bias[8 * g + j], 0.f);
               dst[g] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]),
                                   pack_bf16x2(v[4], v[5]), pack_bf16x2(v[6], v[7]));
             }
@@ -283,7 +287,7 @@ __global__ void __launch_bounds__(kConvThreads)
         __syncwarp();
         if (lane == 0) mbar_arrive(acce0 + 8 * buf);
         const long long o = ((long long)b * a.H + y) * a.W + x;
-        const float rr = __uint_as_float(r[0]) + __ldg(a.bias);
+        const float rr = __uint_as_float(r[0]) + bias[0];
         if constexpr (EPI == kEpiResid) {
           if (in) a.out_f[o] = rr;
         } else {
@@ -553,11 +557,30 @@ static int conv_attr(int* occ) {
   int st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<N, EPI>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             ConvCfg<N>::Smem));
+  // all of the unified L1 as shared memory, so that several CTAs fit on an SM
   if (!st)
-    st = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, conv_tc_kernel<N, EPI>,
-                                                                   kConvThreads, ConvCfg<N>::Smem));
-  if (!st && *occ < 1) st = LCT_ERR_UNSUPPORTED;
-  return st;
+    st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<N, EPI>,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+  // resident CTAs per SM from the kernel's own resources (shared memory, registers, threads);
+  // the runtime's occupancy query answers 1 for this kernel although three fit.  CTAs never
+  // wait on one another, so a grid larger than what is resident only queues.
+  cudaFuncAttributes fa;
+  int dev = 0;
+  cudaDeviceProp pr;
+  if (!st) st = cuda_status(cudaFuncGetAttributes(&fa, conv_tc_kernel<N, EPI>));
+  if (!st) st = cuda_status(cudaGetDevice(&dev));
+  if (!st) st = cuda_status(cudaGetDeviceProperties(&pr, dev));
+  if (st) return st;
+  const size_t smem = ConvCfg<N>::Smem + fa.sharedSizeBytes + pr.reservedSharedMemPerBlock;
+  const int by_smem = (int)(pr.sharedMemPerMultiprocessor / smem);
+  const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+  const int by_regs = pr.regsPerMultiprocessor / (regs_warp * (kConvThreads / 32));
+  const int by_threads = pr.maxThreadsPerMultiProcessor / kConvThreads;
+  int o = by_smem < by_regs ? by_smem : by_regs;
+  o = o < by_threads ? o : by_threads;
+  *occ = o;
+  return o < 1 ? LCT_ERR_UNSUPPORTED : LCT_OK;
 }
 
 static int conv_prepare(int dev) {
