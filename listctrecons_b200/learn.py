@@ -379,10 +379,54 @@ def _train_main(argv=None) -> int:
     return 0
 
 
+def _infer_main(argv=None) -> int:
+    """python -m listctrecons_b200.learn infer [...]: times lct_cnn_infer_volume on a seeded
+    random device volume (CUDA events around each pass after one warm-up pass)."""
+    import argparse
+    import json
+
+    torch = _torch()
+    ap = argparse.ArgumentParser(prog="python -m listctrecons_b200.learn infer")
+    ap.add_argument("--weights", default=None, help="weights file (default: He-init)")
+    ap.add_argument("--nz", type=int, default=16)
+    ap.add_argument("--ny", type=int, default=512)
+    ap.add_argument("--nx", type=int, default=512)
+    ap.add_argument("--max-slices", type=int, default=16)
+    ap.add_argument("--repeat", type=int, default=4)
+    ap.add_argument("--bound", type=float, default=DEFAULT_BOUND / MU_WATER, help="x mu_water")
+    a = ap.parse_args(argv)
+    torch.cuda.set_device(0)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    vol = torch.rand((a.nz, a.ny, a.nx), device="cuda", generator=g)
+    out = torch.empty_like(vol)
+    if a.weights:
+        cnn = cnn_from_weights(a.weights, a.max_slices, a.ny, a.nx)
+    else:
+        cnn = CNN(a.max_slices, a.ny, a.nx, train=False)
+        cnn.set_scales(0.5, 1.0 / MU_WATER)
+    cnn.infer_volume(vol, a.bound * MU_WATER, out=out, count=False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(a.repeat):
+        e0.record()
+        cnn.infer_volume(vol, a.bound * MU_WATER, out=out, count=False)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    n = vol.numel()
+    best = min(ms)
+    print(json.dumps({"volume": [a.nz, a.ny, a.nx], "ms": best, "ms_all": ms,
+                      "tflops": n * 114048 / best / 1e9}), flush=True)
+    return 0
+
+
 if __name__ == "__main__":
     import sys
 
     if len(sys.argv) > 1 and sys.argv[1] == "train":
         sys.exit(_train_main(sys.argv[2:]))
-    print("usage: python -m listctrecons_b200.learn train --out FILE [--pairs N] [--steps N]")
+    if len(sys.argv) > 1 and sys.argv[1] == "infer":
+        sys.exit(_infer_main(sys.argv[2:]))
+    print("usage: python -m listctrecons_b200.learn train --out FILE [--pairs N] [--steps N]\n"
+          "       python -m listctrecons_b200.learn infer [--nz N --ny N --nx N] [--weights F]")
     sys.exit(2)
