@@ -7,7 +7,8 @@
 //   * a bilinear sample is ONE 16-byte load of the 2 x 2 texel block at the clamped sample
 //     origin (quad layout, lct_internal.h); border/clamp addressing lives in the packed data,
 //     so there are no per-texel bounds tests;
-//   * the row coordinate of slice j is one FMA, qhat = zc[j] * k + m, with k and m per view;
+//   * the row coordinate of slice j is one FMA, qhat = zc[j] * k + m (EXACT: h + j * k dz with
+//     the slice index a constant), with k and m per view;
 //   * the pair weights are branch-free selects around one reciprocal;
 //   * views whose window covers every slice of the thread's chunk run an unpredicated loop.
 // EXACT keeps FP64 view trigonometry and full FP32 weights; TEX8 keeps the reference's order
@@ -111,6 +112,16 @@ __device__ __forceinline__ float quad_sample(const float4* __restrict__ qb, int 
   return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
 }
 
+// EXACT sample: u = row coordinate + 2 (texel centres at integers), so floor(u) is the quad row
+__device__ __forceinline__ float quad_sample_exact(const float4* __restrict__ qb, int qcols,
+                                                   int nt, float a, float u) {
+  const float fu = floorf(u);
+  const float b = u - fu;
+  const int j2 = min(max((int)fu, 0), nt + 2);
+  const float4 v = __ldg(qb + j2 * qcols);  // T00, dx, dy, dxy
+  return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
+}
+
 // Column of a sample: clamped origin offset and weight
 template <int INTERP>
 __device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a) {
@@ -142,6 +153,8 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
 
   const float xc = ((float)ix - A.wx) * A.dx;
   const float yc = ((float)iy - A.wy) * A.dy;
+  const float zc0 = ((float)z0 - A.wz) * A.dz;
+  const float wt2 = A.wt + 2.0f;
   float zc[NZ];
 #pragma unroll
   for (int j = 0; j < NZ; ++j) zc[j] = ((float)(z0 + j) - A.wz) * A.dz;
@@ -207,6 +220,35 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       quad_col<INTERP>(-delta_p + A.ws, A.ns, o2, a2);
       const float4* q1 = quads + (long long)ia * A.qstride + o1;
       const float4* q2 = quads + (long long)(ia + A.half) * A.qstride + o2;
+      if constexpr (INTERP == LCT_INTERP_EXACT) {
+        // slice j: qhat = h + j kd (one FMA with a constant j, no per-slice z register);
+        // weights halved around one reciprocal -- the factor 2 is restored, exactly, at the
+        // output
+        const float kd1 = k1 * A.dz, kd2 = k2 * A.dz;
+        const float h1 = fmaf(zc0, k1, m1), h2 = fmaf(zc0, k2, m2);
+        const float u1 = h1 + wt2, u2 = h2 + wt2;
+        auto slice_x = [&](int j) {
+          const float fj = (float)j;
+          const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
+          const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
+          const float r = __fdividef(1.0f, qh1 - qh2);
+          const float in1 = -qh2 * r, in2 = qh1 * r;
+          const float w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
+          const float w2 = out2 ? (out1 ? 0.5f : 0.0f) : (out1 ? 1.0f : in2);
+          const float s1 = quad_sample_exact(q1, A.qcols, A.nt, a1, fmaf(fj, kd1, u1));
+          const float s2 = quad_sample_exact(q2, A.qcols, A.nt, a2, fmaf(fj, kd2, u2));
+          acc[j] = fmaf(w1, s1, fmaf(w2, s2, acc[j]));
+        };
+        if (jlo == 0 && jhi == NZ) {
+#pragma unroll
+          for (int j = 0; j < NZ; ++j) slice_x(j);
+        } else {
+#pragma unroll
+          for (int j = 0; j < NZ; ++j)
+            if (j >= jlo && j < jhi) slice_x(j);
+        }
+        continue;
+      }
       auto slice = [&](int j) {
         const float qh1 = fmaf(zc[j], k1, m1), qh2 = fmaf(zc[j], k2, m2);
         const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
@@ -237,7 +279,9 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       if (j < nzc) {
         const int span = A.a_max[z0 + j] - A.a_min[z0 + j];
         // CUDA/Backprojector.cu:96, evaluated in double (PI is a double literal there)
-        out[j * plane] = span > 0 ? (float)((double)(acc[j] * 2.0f) * kRefPi / (double)(float)span) : 0.0f;
+        // EXACT accumulates halved weights: x4 restores both the halving and the pair doubling
+        const float sc = INTERP == LCT_INTERP_EXACT ? 4.0f : 2.0f;
+        out[j * plane] = span > 0 ? (float)((double)(acc[j] * sc) * kRefPi / (double)(float)span) : 0.0f;
       }
     }
   }
