@@ -251,14 +251,20 @@ int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon
 /* Reconstructs blocks [first_block, first_block + n_blocks_run).  fan: [views][nt][ns] float
    holding fan views from `fan_view0` on (file view numbering, DataOffset included) and at
    least through the run's range (lct_recon_fan_range); host (pinned or pageable) or device.
-   image: [n_blocks_run*32][ny][nx].  Returns after the image is complete (synchronous). */
+   image: [n_blocks_run*32][ny][nx].  Returns after the image is complete (synchronous).
+   Scan mode (fan->parallel rebin, no pre-weighting, parallel BP) with a HOST fan streams: fan
+   views are uploaded in pieces on an internal copy stream while earlier pieces are rebinned,
+   filtered and backprojected slab by slab, and each finished slab is downloaded on a second copy
+   stream (pinned host buffers make the copies asynchronous).  The volume is bit-identical to
+   the device-resident run. */
 int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                   float* image, int image_on_device, lct_stream stream);
 /* Backprojection autotuner (no reference counterpart): times the kernel's slices-per-thread x
    CTAs-per-SM variants on this recon's buffers, keeps the fastest in the recon, and caches it per
    geometry class for the process.  Synchronous; returns the choice. */
 int lct_recon_autotune(lct_recon* r, int* nz, int* minb);
-/* Device-side per-stage time of the last run (ms): h2d, rebin, filter, backproject, d2h. */
+/* Device-side per-stage time of the last run (ms): h2d, rebin, filter, backproject, d2h.  A
+   streamed run reports its whole overlapped span as backprojection and 0 for the others. */
 int lct_recon_last_times(const lct_recon* r, float* ms5);
 /* Fan views [first, first+count) the run reads (h2d bytes = count*nt*ns*4). */
 int lct_recon_fan_range(const lct_recon* r, int64_t* first, int64_t* count);

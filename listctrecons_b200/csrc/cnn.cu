@@ -896,20 +896,25 @@ LCT_API int lct_cnn_last_loss(const lct_cnn* c, double* loss) {
   return st;
 }
 
-LCT_API int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, int nz,
-                                 float bound, int64_t* n_rejected, lct_stream stream) {
+namespace lct {
+
+// Gated inference of the slices [z0, z1) of a volume of nz slices (passes of at most max_slices;
+// the 5-slice inputs read the neighbours, edge slices replicated).  Rejections add to the
+// counter that cnn_reset_rejects clears.
+int cnn_infer_range(lct_cnn* c, const float* d_vol, float* d_out, int nz, int z0, int z1,
+                    float bound, cudaStream_t s) {
   if (!c || !d_vol || !d_out || nz <= 0 || d_vol == d_out || !(bound >= 0.f)) return LCT_ERR_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  int st = cuda_status(cudaMemsetAsync(c->d_rej, 0, sizeof(unsigned long long), s));
+  if (z0 < 0 || z1 > nz || z0 > z1) return LCT_ERR_ARG;
   const long long plane = (long long)c->H * c->W;
-  for (int z0 = 0; z0 < nz && !st; z0 += c->cap) {
-    const int B = nz - z0 < c->cap ? nz - z0 : c->cap;
-    if ((st = run_prep(c, d_vol, 1, z0, nz, B, s))) break;
+  int st = LCT_OK;
+  for (int zb = z0; zb < z1 && !st; zb += c->cap) {
+    const int B = z1 - zb < c->cap ? z1 - zb : c->cap;
+    if ((st = run_prep(c, d_vol, 1, zb, nz, B, s))) break;
     if ((st = run_hidden(c, B, s))) break;
     ConvArgs a;
     last_bias_and_args(c, a);
-    a.out_f = d_out + (size_t)z0 * plane;
-    a.xc = d_vol + (size_t)z0 * plane;
+    a.out_f = d_out + (size_t)zb * plane;
+    a.xc = d_vol + (size_t)zb * plane;
     a.calib = c->calib;
     a.inv_scale = 1.f / c->in_scale;
     a.bound = bound;
@@ -917,6 +922,23 @@ LCT_API int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, i
     st = launch_conv<16, kEpiGate>(c->m_act[act_in(c, kCnnLayers - 1)], c->m_wf[kCnnLayers - 1],
                                    a, B, c->device, c->sms, s);
   }
+  return st;
+}
+
+int cnn_reset_rejects(lct_cnn* c, cudaStream_t s) {
+  return cuda_status(cudaMemsetAsync(c->d_rej, 0, sizeof(unsigned long long), s));
+}
+
+int cnn_passes(const lct_cnn* c, int nslices) { return (nslices + c->cap - 1) / c->cap; }
+
+}  // namespace lct
+
+LCT_API int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, int nz,
+                                 float bound, int64_t* n_rejected, lct_stream stream) {
+  if (!c || !d_vol || !d_out || nz <= 0 || d_vol == d_out || !(bound >= 0.f)) return LCT_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int st = cnn_reset_rejects(c, s);
+  if (!st) st = cnn_infer_range(c, d_vol, d_out, nz, 0, nz, bound, s);
   if (!st && n_rejected) {
     unsigned long long v = 0;
     st = cuda_status(cudaMemcpyAsync(&v, c->d_rej, sizeof(v), cudaMemcpyDeviceToHost, s));

@@ -12,6 +12,7 @@
 //         block_proj_start + add_projections (CUDA/Backprojector.cu:145)
 //   img   n_blocks_run * 32 slices, block b at slice 32 b (CUDA/Backprojector.cu:158)
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -43,6 +44,10 @@ static void free_recon(lct_recon* r) {
     if (e) cudaEventDestroy(e);
   for (auto& e : r->ev_cnn)
     if (e) cudaEventDestroy(e);
+  for (auto& e : r->sev)
+    if (e) cudaEventDestroy(e);
+  if (r->s_up) cudaStreamDestroy(r->s_up);
+  if (r->s_down) cudaStreamDestroy(r->s_down);
   delete r;
 }
 
@@ -461,6 +466,144 @@ int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s) {
 
 }  // namespace lct
 
+// Scan mode from a HOST fan buffer with the copies overlapped: slabs are taken in the order their
+// view windows end; for each, the fan views up to that end are uploaded on a copy stream, the
+// new global views are rebinned, filtered and packed on the compute stream, and the slab is
+// backprojected (the new views in pieces of at most 512, each uploaded, then rebinned, filtered
+// and packed, so the compute starts after the first piece); its volume -- or, with a network
+// attached, the corrected slab once the slabs
+// on either side are backprojected -- is downloaded on a second copy stream.  Every view is
+// uploaded, rebinned and filtered once by the same kernels as the unstreamed run, so the volume
+// is bit-identical to it.
+static bool streamable(const lct_recon* r) {
+  return r->o.mode == LCT_MODE_SCAN && r->o.rebinner == LCT_REBIN_FAN2PAR &&
+         r->o.preweight == LCT_PW_NONE && r->o.backprojector == LCT_BP_PAR;
+}
+
+constexpr long long kStreamPiece = 512;  // global views per upload / rebin / filter piece
+
+static int run_streaming(lct_recon* r, const float* fan_host, long long skip, float* d_img,
+                         float* d_out, float* image_host, cudaStream_t s) {
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  const int nb = r->info.n_blocks_run;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  const long long plane = r->plane;
+  int st;
+  if (!r->s_up && (st = cuda_status(cudaStreamCreateWithFlags(&r->s_up, cudaStreamNonBlocking))))
+    return st;
+  if (!r->s_down &&
+      (st = cuda_status(cudaStreamCreateWithFlags(&r->s_down, cudaStreamNonBlocking))))
+    return st;
+  // start, downloads done, per slab: backprojected, corrected; one per uploaded piece
+  const long long n_pieces = r->g_count / kStreamPiece + nb + 1;
+  const size_t n_ev = 2 + 2 * (size_t)nb + (size_t)n_pieces;
+  while (r->sev.size() < n_ev) {
+    cudaEvent_t e;
+    if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return st;
+    r->sev.push_back(e);
+  }
+  cudaEvent_t ev_start = r->sev[0], ev_down = r->sev[1];
+  cudaEvent_t* ev_bp = r->sev.data() + 2;
+  cudaEvent_t* ev_cnn = ev_bp + nb;
+  cudaEvent_t* ev_up = ev_cnn + nb;
+  long long piece = 0;
+  // the copy streams start after everything already queued on s (an earlier run included)
+  if ((st = cuda_status(cudaEventRecord(ev_start, s)))) return st;
+  if ((st = cuda_status(cudaStreamWaitEvent(r->s_up, ev_start, 0)))) return st;
+  if ((st = cuda_status(cudaStreamWaitEvent(r->s_down, ev_start, 0)))) return st;
+
+  // fan views a range of global views reads (the scan rebin's column shifts, in FP64)
+  const double smax = (((double)(g.ns - 1) - (double)g.ws) * (double)g.ds / (double)g.dso) /
+                      (double)g.orbit;
+  const long long shift_hi = (long long)std::floor(smax) + 1;
+  std::vector<int> order(nb);
+  std::vector<long long> gend(nb);
+  for (int b = 0; b < nb; ++b) {
+    order[b] = b;
+    gend[b] = r->blocks[b].block_proj_start + g.add_projections + g.n_angle;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return gend[x] < gend[y]; });
+  const int addr0 = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  const int packed = addr0;
+  long long done = r->g_first, up = 0;  // global views rebinned so far; fan views uploaded
+  std::vector<char> bp_done(nb, 0), cnn_done(nb, 0);
+  auto download = [&](int b, const float* src, cudaEvent_t after) -> int {
+    if (!image_host) return LCT_OK;
+    int e = cuda_status(cudaStreamWaitEvent(r->s_down, after, 0));
+    if (!e)
+      e = cuda_status(cudaMemcpyAsync(image_host + b * slab, src + b * slab, sizeof(float) * slab,
+                                      cudaMemcpyDeviceToHost, r->s_down));
+    return e;
+  };
+  for (int k = 0; k < nb; ++k) {
+    const int b = order[k];
+    const long long slab_end = std::min(gend[b], r->g_first + r->g_count);
+    while (slab_end > done) {
+      const long long target = std::min(slab_end, done + kStreamPiece);
+      const long long need = std::min(r->fan_count, target - 1 + shift_hi + 1 - r->fan_first);
+      if (need > up) {
+        if ((st = cuda_status(cudaMemcpyAsync(r->d_fan + up * plane, fan_host + (skip + up) * plane,
+                                              sizeof(float) * (need - up) * plane,
+                                              cudaMemcpyHostToDevice, r->s_up))))
+          return st;
+        up = need;
+      }
+      if (piece >= n_pieces) return LCT_ERR_ARG;  // cannot happen: pieces are counted above
+      if ((st = cuda_status(cudaEventRecord(ev_up[piece], r->s_up)))) return st;
+      if ((st = cuda_status(cudaStreamWaitEvent(s, ev_up[piece], 0)))) return st;
+      ++piece;
+      const long long v0 = done - r->g_first, nv = target - done;
+      float* par = r->d_par + v0 * plane;
+      if ((st = launch_rebin_fan2par_scan(g, r->d_fan, r->fan_first, r->fan_count, par, done, nv,
+                                          r->o.interp, addr0, s)))
+        return st;
+      r->launches++;
+      if (r->o.filter_mode != LCT_FILTER_FP32)
+        st = tc_filter(g.ns, par, nv * g.nt, r->d_tc, r->tc_rows, r->o.filter_mode, s);
+      else
+        st = launch_filter_rows(g.ns, r->d_h, par, nv * g.nt, LCT_FILTER_FP32, s);
+      if (st) return st;
+      r->launches += filter_launches(r->o.filter_mode);
+      if (r->quads) {
+        if ((st = launch_quad_pack(par, nv, g.ns, g.nt, packed,
+                                   r->d_quad + v0 * quad_view_elems(g.ns, g.nt), s)))
+          return st;
+        r->launches++;
+      }
+      done = target;
+    }
+    BpLaunch L;
+    recon_bp_launch(r, b, b + 1, d_img, L);
+    const int addr = block_addr(r, b);
+    st = (r->quads && addr == packed) ? launch_bp_par_quads(g, ig, L, r->d_quad, s)
+                                      : launch_bp_par(g, ig, L, s);
+    if (st) return st;
+    r->launches++;
+    bp_done[b] = 1;
+    if ((st = cuda_status(cudaEventRecord(ev_bp[b], s)))) return st;
+    if (!r->cnn) {
+      if ((st = download(b, d_out, ev_bp[b]))) return st;
+      continue;
+    }
+    // corrected slabs whose 5-slice inputs are now all backprojected
+    for (int c = std::max(0, b - 1); c <= std::min(nb - 1, b + 1); ++c) {
+      if (cnn_done[c] || !bp_done[c] || (c > 0 && !bp_done[c - 1]) || (c + 1 < nb && !bp_done[c + 1]))
+        continue;
+      if ((st = cnn_infer_range(r->cnn, d_img, d_out, nb * kBlockSlices, c * kBlockSlices,
+                                (c + 1) * kBlockSlices, r->cnn_bound, s)))
+        return st;
+      r->launches += 9 * cnn_passes(r->cnn, kBlockSlices);
+      cnn_done[c] = 1;
+      if ((st = cuda_status(cudaEventRecord(ev_cnn[c], s)))) return st;
+      if ((st = download(c, d_out, ev_cnn[c]))) return st;
+    }
+  }
+  // the compute stream ends after the last download
+  if ((st = cuda_status(cudaEventRecord(ev_down, r->s_down)))) return st;
+  return cuda_status(cudaStreamWaitEvent(s, ev_down, 0));
+}
+
 LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                           float* image, int image_on_device, lct_stream stream) {
   if (!r || !fan || !image) return LCT_ERR_ARG;
@@ -471,11 +614,33 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
   const long long off = r->info.data_offset;
   int st;
   r->launches = 0;
+  r->streamed = false;
   if ((st = cuda_status(cudaEventRecord(r->ev[0], s)))) return st;
 
   // fan views needed by the run (the union of the blocks' windows)
   const float* d_fan;
   const long long skip = r->fan_first + off - fan_view0;  // views before the run's first
+  if (!fan_on_device && streamable(r)) {
+    // host fan: copies overlapped with the compute; one span reported as backprojection
+    float* d_out = image_on_device ? image : r->d_img;
+    float* d_img = r->cnn ? r->d_plain : d_out;
+    r->streamed = true;
+    if (r->cnn && (st = cnn_reset_rejects(r->cnn, s))) return st;
+    for (int i = 1; i < 4; ++i)
+      if ((st = cuda_status(cudaEventRecord(r->ev[i], s)))) return st;
+    if ((st = run_streaming(r, fan + 0, skip, d_img, d_out, image_on_device ? nullptr : image, s)))
+      return st;
+    if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
+    if ((st = cuda_status(cudaEventRecord(r->ev[5], s)))) return st;
+    if ((st = cuda_status(cudaEventSynchronize(r->ev[5])))) return st;
+    for (int i = 0; i < 5; ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r->ev[i], r->ev[i + 1]);
+      r->times[i] = ms;
+    }
+    r->cnn_ms = 0.f;  // interleaved with the backprojection: not separable
+    return LCT_OK;
+  }
   if (fan_on_device) {
     d_fan = fan + skip * r->plane;
   } else {

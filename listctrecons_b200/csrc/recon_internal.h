@@ -28,6 +28,10 @@ struct lct_recon {
   float* d_plain = nullptr;  // plain FDK volume when the learned correction runs
   cudaEvent_t ev_cnn[2] = {};
   float cnn_ms = 0.f;
+  // streaming runs from host fan buffers: copy streams and per-slab events (created on first use)
+  cudaStream_t s_up = nullptr, s_down = nullptr;
+  std::vector<cudaEvent_t> sev;
+  bool streamed = false;  // the last run overlapped its copies with the compute
   int device = 0;
   long long voxel_updates = 0;
   int launches = 0;
@@ -40,4 +44,9 @@ int recon_stage_filter(lct_recon* r, cudaStream_t s);
 int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s);
 void recon_bp_launch(const lct_recon* r, int b0, int b1, float* d_img, BpLaunch& L);
 bool recon_bp_quads_all(const lct_recon* r);
+// learned correction of slices [z0, z1) of an nz-slice volume (cnn.cu)
+int cnn_infer_range(lct_cnn* c, const float* d_vol, float* d_out, int nz, int z0, int z1,
+                    float bound, cudaStream_t s);
+int cnn_reset_rejects(lct_cnn* c, cudaStream_t s);
+int cnn_passes(const lct_cnn* c, int nslices);  // kernel passes of prep + 8 convolutions
 }  // namespace lct

@@ -106,7 +106,8 @@ def test_host_buffers_end_to_end(scan):
     r.run(host_in, host_out)
     assert np.array_equal(host_out.numpy(), dev)
     t = r.last_times()
-    assert t["h2d"] > 0 and t["backproject"] > 0
+    # streamed (host fan, scan mode): the copies overlap the compute, reported as one span
+    assert t["backproject"] > 0 and t["h2d"] < 0.1 * t["backproject"]
 
 
 def _write(scan, tmp_path):
