@@ -44,6 +44,7 @@ struct BpQuadArgs {
   int half;
   int zchunks;
   int gx, gy, gz;  // tile grid (work-list decoding)
+  int view_lo, view_hi, part;  // BpLaunch::view_lo / view_hi / part
   int slab_view[kBpMaxSlabs];
   int slab_z0[kBpMaxSlabs];
   int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
@@ -139,7 +140,7 @@ __device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a
 
 // One tile: voxel columns [bx*32, +32) x [by*8, +8), slab/slice chunk bz.  Called with
 // CTA-uniform arguments by every thread of a 256-thread CTA.
-template <int NZ, int INTERP>
+template <int NZ, int INTERP, bool PART>
 __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by, int bz) {
   __shared__ float s_c1[kQVB], s_s1[kQVB], s_c2[kQVB], s_s2[kQVB];
   __shared__ int s_jlo[kQVB], s_jhi[kQVB];
@@ -164,6 +165,10 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
     vlo = min(vlo, A.a_min[z0 + j]);
     vhi = max(vhi, A.a_mid[z0 + j]);
   }
+  if (PART) {
+    vlo = max(vlo, A.view_lo);
+    vhi = min(vhi, A.view_hi);
+  }
   const float4* quads = A.quads + (long long)A.slab_view[slab] * A.qstride;
   const float* betas = A.betas + A.slab_view[slab];
   const float wt = A.wt;
@@ -171,6 +176,12 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   float acc[NZ];
 #pragma unroll
   for (int j = 0; j < NZ; ++j) acc[j] = 0.0f;
+  if (PART && A.part >= kBpMiddle && ix < A.nx && iy < A.ny) {  // continue earlier parts' sums
+    const float* in = A.img + ((long long)(A.slab_z0[slab] + z0) * A.ny + iy) * A.nx + ix;
+#pragma unroll
+    for (int j = 0; j < NZ; ++j)
+      if (j < nzc) acc[j] = in[j * (long long)A.nx * A.ny];
+  }
 
   for (int vb = vlo; vb < vhi; vb += kQVB) {
     __syncthreads();
@@ -274,9 +285,12 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   if (ix < A.nx && iy < A.ny) {
     float* out = A.img + ((long long)(A.slab_z0[slab] + z0) * A.ny + iy) * A.nx + ix;
     const long long plane = (long long)A.nx * A.ny;
+    const bool raw = PART && (A.part == kBpFirst || A.part == kBpMiddle);  // more parts follow
 #pragma unroll
     for (int j = 0; j < NZ; ++j) {
-      if (j < nzc) {
+      if (j < nzc && raw) {
+        out[j * plane] = acc[j];
+      } else if (j < nzc) {
         const int span = A.a_max[z0 + j] - A.a_min[z0 + j];
         // CUDA/Backprojector.cu:96, evaluated in double (PI is a double literal there)
         // EXACT accumulates halved weights: x4 restores both the halving and the pair doubling
@@ -287,9 +301,11 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   }
 }
 
-template <int NZ, int INTERP, int MINB>
+// PART: a view range of the slabs with raw sums carried in img (BpLaunch::part); the whole-
+// launch instantiation has none of that code
+template <int NZ, int INTERP, int MINB, bool PART>
 __global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_constant__ BpQuadArgs A) {
-  bp_quad_tile<NZ, INTERP>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+  bp_quad_tile<NZ, INTERP, PART>(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Persistent work list over several scans: item i belongs to the scan s with
@@ -324,7 +340,7 @@ __global__ void __launch_bounds__(kQTX* kQTY, MINB)
     const int bx = local % sA.gx;
     const int by = (local / sA.gx) % sA.gy;
     const int bz = local / (sA.gx * sA.gy);
-    bp_quad_tile<NZ, INTERP>(sA, bx, by, bz);
+    bp_quad_tile<NZ, INTERP, false>(sA, bx, by, bz);
   }
 }
 
@@ -388,6 +404,10 @@ static int build_bp_quad_args(const lct_geom& g, const lct_img& ig, const BpLaun
   a.gx = (ig.nx + kQTX - 1) / kQTX;
   a.gy = (ig.ny + kQTY - 1) / kQTY;
   a.gz = L.n_slabs * a.zchunks;
+  if (L.part < kBpWhole || L.part > kBpLast || L.view_lo > L.view_hi) return LCT_ERR_ARG;
+  a.view_lo = L.view_lo;
+  a.view_hi = L.view_hi;
+  a.part = L.part;
   if (a.gz > 65535) return LCT_ERR_ARG;
   return LCT_OK;
 }
@@ -403,10 +423,13 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
   const bool tex = L.interp == LCT_INTERP_TEX8;
   int minb = L.minb;
   if (minb < 1 || minb > 4) minb = 4;  // measured best on B200 (4 CTAs x 256 threads per SM)
-#define LCT_BPQ(NZV, MB)                                                                  \
-  do {                                                                                    \
-    if (tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB><<<grid, block, 0, s>>>(a);          \
-    else bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB><<<grid, block, 0, s>>>(a);             \
+  const bool part = L.part != kBpWhole || L.view_lo > 0 || L.view_hi < (1 << 30);
+#define LCT_BPQ(NZV, MB)                                                                      \
+  do {                                                                                        \
+    if (part && tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB, true><<<grid, block, 0, s>>>(a);  \
+    else if (part) bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB, true><<<grid, block, 0, s>>>(a);   \
+    else if (tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB, false><<<grid, block, 0, s>>>(a);    \
+    else bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB, false><<<grid, block, 0, s>>>(a);            \
   } while (0)
 #define LCT_BPQ_NZ(NZV)            \
   do {                             \

@@ -63,7 +63,14 @@ struct BpLaunch {
   int interp, addr;
   int nz_thread;       // slices per thread (8, 16, 32; 0 = choose)
   int minb = 0;        // quad kernel: resident CTAs per SM the register budget targets (0 = 4)
+  // quad kernel only: a part of the slabs' views, [view_lo, view_hi) in slab-local indices,
+  // carried between parts as raw FP32 sums in img (part kBpWhole / First / Middle / Last); the
+  // parts of one slab run in order on one stream and sum every view in the same sequence as a
+  // whole launch
+  int view_lo = 0, view_hi = 1 << 30;
+  int part = 0;
 };
+enum BpPart : int { kBpWhole = 0, kBpFirst = 1, kBpMiddle = 2, kBpLast = 3 };
 int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaStream_t s);
 
 // Filtered views in quad layout for the backprojector.  Per view, entry (j, i) for

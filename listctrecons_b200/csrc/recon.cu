@@ -46,8 +46,8 @@ static void free_recon(lct_recon* r) {
     if (e) cudaEventDestroy(e);
   for (auto& e : r->sev)
     if (e) cudaEventDestroy(e);
-  if (r->s_up) cudaStreamDestroy(r->s_up);
-  if (r->s_down) cudaStreamDestroy(r->s_down);
+  for (cudaStream_t x : {r->s_up, r->s_down, r->s_bp[0], r->s_bp[1], r->s_cnn})
+    if (x) cudaStreamDestroy(x);
   delete r;
 }
 
@@ -469,9 +469,9 @@ int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s) {
 // Scan mode from a HOST fan buffer with the copies overlapped: slabs are taken in the order their
 // view windows end; for each, the fan views up to that end are uploaded on a copy stream, the
 // new global views are rebinned, filtered and packed on the compute stream, and the slab is
-// backprojected (the new views in pieces of at most 512, each uploaded, then rebinned, filtered
-// and packed, so the compute starts after the first piece); its volume -- or, with a network
-// attached, the corrected slab once the slabs
+// backprojected on one of two alternating streams, the first slab in parts as its views land
+// (the new views come in pieces of at most 512, each uploaded, then rebinned, filtered and
+// packed); its volume -- or, with a network attached, the corrected slab once the slabs
 // on either side are backprojected -- is downloaded on a second copy stream.  Every view is
 // uploaded, rebinned and filtered once by the same kernels as the unstreamed run, so the volume
 // is bit-identical to it.
@@ -490,38 +490,41 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
   const long long plane = r->plane;
   int st;
-  if (!r->s_up && (st = cuda_status(cudaStreamCreateWithFlags(&r->s_up, cudaStreamNonBlocking))))
-    return st;
-  if (!r->s_down &&
-      (st = cuda_status(cudaStreamCreateWithFlags(&r->s_down, cudaStreamNonBlocking))))
-    return st;
-  // start, downloads done, per slab: backprojected, corrected; one per uploaded piece
+  cudaStream_t* aux[5] = {&r->s_up, &r->s_down, &r->s_bp[0], &r->s_bp[1], &r->s_cnn};
+  for (auto* a : aux)
+    if (!*a && (st = cuda_status(cudaStreamCreateWithFlags(a, cudaStreamNonBlocking)))) return st;
+  // events: start, 4 stream ends, per slab: views ready, backprojected, corrected; per piece:
+  // uploaded, packed
   const long long n_pieces = r->g_count / kStreamPiece + nb + 1;
-  const size_t n_ev = 2 + 2 * (size_t)nb + (size_t)n_pieces;
+  const size_t n_ev = 5 + 3 * (size_t)nb + 2 * (size_t)n_pieces;
   while (r->sev.size() < n_ev) {
     cudaEvent_t e;
     if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return st;
     r->sev.push_back(e);
   }
-  cudaEvent_t ev_start = r->sev[0], ev_down = r->sev[1];
-  cudaEvent_t* ev_bp = r->sev.data() + 2;
+  cudaEvent_t ev_start = r->sev[0];
+  cudaEvent_t* ev_end = r->sev.data() + 1;
+  cudaEvent_t* ev_views = ev_end + 4;
+  cudaEvent_t* ev_bp = ev_views + nb;
   cudaEvent_t* ev_cnn = ev_bp + nb;
   cudaEvent_t* ev_up = ev_cnn + nb;
+  cudaEvent_t* ev_packed = ev_up + n_pieces;
   long long piece = 0;
-  // the copy streams start after everything already queued on s (an earlier run included)
+  // the other streams start after everything already queued on s (an earlier run included)
   if ((st = cuda_status(cudaEventRecord(ev_start, s)))) return st;
-  if ((st = cuda_status(cudaStreamWaitEvent(r->s_up, ev_start, 0)))) return st;
-  if ((st = cuda_status(cudaStreamWaitEvent(r->s_down, ev_start, 0)))) return st;
+  for (int i = 0; i < 5; ++i)
+    if ((st = cuda_status(cudaStreamWaitEvent(*aux[i], ev_start, 0)))) return st;
 
   // fan views a range of global views reads (the scan rebin's column shifts, in FP64)
   const double smax = (((double)(g.ns - 1) - (double)g.ws) * (double)g.ds / (double)g.dso) /
                       (double)g.orbit;
   const long long shift_hi = (long long)std::floor(smax) + 1;
   std::vector<int> order(nb);
-  std::vector<long long> gend(nb);
+  std::vector<long long> gfirst(nb), gend(nb);
   for (int b = 0; b < nb; ++b) {
     order[b] = b;
-    gend[b] = r->blocks[b].block_proj_start + g.add_projections + g.n_angle;
+    gfirst[b] = r->blocks[b].block_proj_start + g.add_projections;
+    gend[b] = gfirst[b] + g.n_angle;
   }
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return gend[x] < gend[y]; });
   const int addr0 = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
@@ -536,12 +539,30 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
                                       cudaMemcpyDeviceToHost, r->s_down));
     return e;
   };
+  auto bp = [&](int b, int lo, int hi, int part, cudaStream_t sb) -> int {
+    BpLaunch L;
+    recon_bp_launch(r, b, b + 1, d_img, L);
+    L.view_lo = lo;
+    L.view_hi = hi;
+    L.part = part;
+    const int addr = block_addr(r, b);
+    const int e = (r->quads && addr == packed) ? launch_bp_par_quads(g, ig, L, r->d_quad, sb)
+                                               : launch_bp_par(g, ig, L, sb);
+    if (!e) r->launches++;
+    return e;
+  };
   for (int k = 0; k < nb; ++k) {
     const int b = order[k];
+    cudaStream_t sb = r->s_bp[k & 1];
+    // the first slab is backprojected in parts as its views arrive (the others' windows are
+    // complete by the time their turn comes); only the quad kernel carries parts
+    const bool split = k == 0 && r->quads && block_addr(r, b) == packed;
     const long long slab_end = std::min(gend[b], r->g_first + r->g_count);
+    int bp_lo = 0, parts = 0;
     while (slab_end > done) {
       const long long target = std::min(slab_end, done + kStreamPiece);
       const long long need = std::min(r->fan_count, target - 1 + shift_hi + 1 - r->fan_first);
+      if (piece >= n_pieces) return LCT_ERR_ARG;  // cannot happen: pieces are counted above
       if (need > up) {
         if ((st = cuda_status(cudaMemcpyAsync(r->d_fan + up * plane, fan_host + (skip + up) * plane,
                                               sizeof(float) * (need - up) * plane,
@@ -549,10 +570,8 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
           return st;
         up = need;
       }
-      if (piece >= n_pieces) return LCT_ERR_ARG;  // cannot happen: pieces are counted above
       if ((st = cuda_status(cudaEventRecord(ev_up[piece], r->s_up)))) return st;
       if ((st = cuda_status(cudaStreamWaitEvent(s, ev_up[piece], 0)))) return st;
-      ++piece;
       const long long v0 = done - r->g_first, nv = target - done;
       float* par = r->d_par + v0 * plane;
       if ((st = launch_rebin_fan2par_scan(g, r->d_fan, r->fan_first, r->fan_count, par, done, nv,
@@ -572,36 +591,52 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
         r->launches++;
       }
       done = target;
+      if ((st = cuda_status(cudaEventRecord(ev_packed[piece], s)))) return st;
+      ++piece;
+      // a pair starting at local view ia also reads its conjugate ia + half: a part takes the
+      // pair starts whose conjugates are packed too
+      const long long local = std::min<long long>(done - gfirst[b], g.n_angle);
+      const int avail = (int)std::max<long long>(local - g.n_proj_turn / 2, 0);
+      if (split && done < slab_end && avail > bp_lo) {
+        if ((st = cuda_status(cudaStreamWaitEvent(sb, ev_packed[piece - 1], 0)))) return st;
+        if ((st = bp(b, bp_lo, avail, parts ? kBpMiddle : kBpFirst, sb))) return st;
+        bp_lo = avail;
+        ++parts;
+      }
     }
-    BpLaunch L;
-    recon_bp_launch(r, b, b + 1, d_img, L);
-    const int addr = block_addr(r, b);
-    st = (r->quads && addr == packed) ? launch_bp_par_quads(g, ig, L, r->d_quad, s)
-                                      : launch_bp_par(g, ig, L, s);
-    if (st) return st;
-    r->launches++;
+    // every view of the slab's window is packed
+    if ((st = cuda_status(cudaEventRecord(ev_views[k], s)))) return st;
+    if ((st = cuda_status(cudaStreamWaitEvent(sb, ev_views[k], 0)))) return st;
+    if ((st = parts ? bp(b, bp_lo, g.n_angle, kBpLast, sb) : bp(b, 0, 1 << 30, kBpWhole, sb)))
+      return st;
     bp_done[b] = 1;
-    if ((st = cuda_status(cudaEventRecord(ev_bp[b], s)))) return st;
+    if ((st = cuda_status(cudaEventRecord(ev_bp[b], sb)))) return st;
     if (!r->cnn) {
       if ((st = download(b, d_out, ev_bp[b]))) return st;
       continue;
     }
-    // corrected slabs whose 5-slice inputs are now all backprojected
+    // corrected slabs whose 5-slice inputs are now all backprojected (one stream: the network's
+    // workspace is shared by its passes)
     for (int c = std::max(0, b - 1); c <= std::min(nb - 1, b + 1); ++c) {
       if (cnn_done[c] || !bp_done[c] || (c > 0 && !bp_done[c - 1]) || (c + 1 < nb && !bp_done[c + 1]))
         continue;
+      for (int n = std::max(0, c - 1); n <= std::min(nb - 1, c + 1); ++n)
+        if ((st = cuda_status(cudaStreamWaitEvent(r->s_cnn, ev_bp[n], 0)))) return st;
       if ((st = cnn_infer_range(r->cnn, d_img, d_out, nb * kBlockSlices, c * kBlockSlices,
-                                (c + 1) * kBlockSlices, r->cnn_bound, s)))
+                                (c + 1) * kBlockSlices, r->cnn_bound, r->s_cnn)))
         return st;
       r->launches += 9 * cnn_passes(r->cnn, kBlockSlices);
       cnn_done[c] = 1;
-      if ((st = cuda_status(cudaEventRecord(ev_cnn[c], s)))) return st;
+      if ((st = cuda_status(cudaEventRecord(ev_cnn[c], r->s_cnn)))) return st;
       if ((st = download(c, d_out, ev_cnn[c]))) return st;
     }
   }
-  // the compute stream ends after the last download
-  if ((st = cuda_status(cudaEventRecord(ev_down, r->s_down)))) return st;
-  return cuda_status(cudaStreamWaitEvent(s, ev_down, 0));
+  // s ends after every other stream
+  for (int i = 1; i < 5; ++i) {
+    if ((st = cuda_status(cudaEventRecord(ev_end[i - 1], *aux[i])))) return st;
+    if ((st = cuda_status(cudaStreamWaitEvent(s, ev_end[i - 1], 0)))) return st;
+  }
+  return LCT_OK;
 }
 
 LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,

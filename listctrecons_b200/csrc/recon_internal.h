@@ -29,7 +29,7 @@ struct lct_recon {
   cudaEvent_t ev_cnn[2] = {};
   float cnn_ms = 0.f;
   // streaming runs from host fan buffers: copy streams and per-slab events (created on first use)
-  cudaStream_t s_up = nullptr, s_down = nullptr;
+  cudaStream_t s_up = nullptr, s_down = nullptr, s_bp[2] = {}, s_cnn = nullptr;
   std::vector<cudaEvent_t> sev;
   bool streamed = false;  // the last run overlapped its copies with the compute
   int device = 0;
