@@ -628,6 +628,7 @@ def run_ours(args, rank, world, dist):
                 interp=capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT,
                 addr=capi.ADDR_BORDER, bp_nz=args.bp_nz, bp_minb=args.bp_minb)
     rec = Reconstruction(plan, **opts)
+    tuned = rec.autotune() if args.bp_nz == -1 else None  # the choice cached at create
     st = rec.stats()
     f0, fc = rec.fan_first, rec.fan_count
     log(f"[rank {rank}] views {f0}..{f0 + fc} of {geo.readings}, blocks "
@@ -731,7 +732,10 @@ def run_ours(args, rank, world, dist):
         "data": "synthetic (seeded 30-ellipsoid phantom, analytic helical scan + Poisson I0=1e5, simulated on the GPU)",
         "config": {"workload": w["label"], "volume": [nb * 32, ig.ny, ig.nx],
                    "views_read": fc, "mode": args.mode, "interp": args.interp,
-                   "filter": args.filter, "bp_nz": args.bp_nz or "auto", "bp_minb": args.bp_minb or "auto",
+                   "filter": args.filter,
+                   "bp_nz": tuned[0] if tuned else (args.bp_nz or "auto"),
+                   "bp_minb": tuned[1] if tuned else (args.bp_minb or "auto"),
+                   "bp_tuning": "autotuned at create" if tuned else "fixed",
                    "l2": "inputs larger than L2 (fan %.2f GB, filtered views %.2f GB)" % (
                        fc * g.nt * g.ns * 4 / 1e9, st.rebinned_views * g.nt * g.ns * 4 / 1e9),
                    "parallelism": f"slab shards x{world}"},
@@ -783,7 +787,8 @@ def main() -> int:
     ap.add_argument("--interp", default="exact", choices=["tex8", "exact"],
                     help="exact: FP64 geometry, full FP32 weights (the FP64-oracle accuracy bar); "
                          "tex8: the reference's texture sampling (drop-in parity)")
-    ap.add_argument("--bp-nz", type=int, default=0)
+    ap.add_argument("--bp-nz", type=int, default=0,
+                    help="slices per backprojection thread: 4, 8, 16; 0 = default; -1 = autotune")
     ap.add_argument("--bp-minb", type=int, default=0)
     ap.add_argument("--blocks", type=int, default=0, help="override the blocks per GPU (profiling)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
