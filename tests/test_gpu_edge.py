@@ -1,0 +1,72 @@
+"""Edge cases on the GPU: a ragged geometry (odd column count, 7 detector rows, a 45 x 37 image,
+slab widths that are no multiple of the tiles) through the whole pipeline in every filter mode
+and from host and device buffers against the FP64 oracle, and empty inputs."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from listctrecons_b200 import capi
+from listctrecons_b200.recon import Plan, Reconstruction
+from listctrecons_b200.scan import Phantom, ScanGeometry, simulate_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ragged(cuda):
+    geo = ScanGeometry(ns=97, nt=7, ds=1.0, dt=1.1, npt=130, pitch=0.9, nx=45, ny=37, dx=1.1,
+                       dz=0.9).with_blocks(2)
+    p = Plan(geo)
+    zs = [b.block_start for b in p.blocks] + [b.block_end for b in p.blocks]
+    ph = Phantom.random(6, seed=21, fov_radius=20.0, z_lo=min(zs), z_hi=max(zs), semi=(2.0, 9.0))
+    fan = simulate_gpu(geo, ph, i0=1e5, seed=22)
+    return p, fan
+
+
+def _oracle(p, fan):
+    g, ig = p.info.ctg, p.info.ig
+    h = orc.ramp_taps(g.ns, g.ds)
+    out = []
+    for bi in p.blocks[: p.info.n_blocks_run]:
+        blk = fan[bi.block_proj_start: bi.block_proj_start + g.n_angle_add]
+        par = orc.rebin_fan2par(g, blk, orc.EXACT, orc.BORDER).astype(np.float32)
+        f = orc.filter_rows(h, par.reshape(-1, g.ns), mode=0).reshape(par.shape).astype(np.float32)
+        betas = p.angles32[bi.block_proj_start + g.add_projections:][: g.n_angle]
+        out.append(orc.bp_par(g, ig, betas, f, orc.EXACT, orc.BORDER))
+    return np.concatenate(out, 0)
+
+
+@pytest.mark.parametrize("fmode", [capi.FILTER_FP32, capi.FILTER_BF16X6])
+@pytest.mark.parametrize("mode", [capi.MODE_SCAN, capi.MODE_BLOCK])
+def test_ragged_geometry_matches_fp64_oracle(ragged, fmode, mode):
+    import torch
+
+    p, fan = ragged
+    ref = _oracle(p, fan.cpu().numpy())
+    rec = Reconstruction(p, mode=mode, interp=capi.INTERP_EXACT, filter_mode=fmode)
+    img = rec.run(fan).cpu().numpy()
+    err = orc.rel_l2(img, ref)
+    print(f"ragged mode={mode} filter={fmode}: rel_l2 {err:.2e}")
+    assert err < 1e-4  # the FP32-volume bar
+    host = torch.empty(rec.image_shape, dtype=torch.float32).pin_memory()
+    rec.run(fan.cpu().pin_memory(), host)
+    assert np.array_equal(host.numpy(), img)
+
+
+def test_empty_inputs(cuda):
+    import torch
+
+    lib = capi.load()
+    h = torch.zeros(2 * 33, device="cuda")
+    rows = torch.zeros(33, device="cuda")
+    # zero rows: nothing to filter, in every mode
+    for m in (capi.FILTER_FP32, capi.FILTER_BF16X3, capi.FILTER_BF16X6):
+        assert lib.lct_filter_rows(33, h.data_ptr(), rows.data_ptr(), 0, m, None) == capi.LCT_OK
+    # an empty view range simulates nothing
+    ell = torch.zeros(16, dtype=torch.float64, device="cuda")
+    ang = torch.zeros(4, dtype=torch.float64, device="cuda")
+    fan = torch.zeros(4 * 2 * 8, device="cuda")
+    assert lib.lct_sim_project(ell.data_ptr(), 1, 8, 2, 1.0, 1.0, 3.5, 0.5, 570.0, ang.data_ptr(),
+                               ang.data_ptr(), 2, 2, 1e5, 1, fan.data_ptr(), None) == capi.LCT_OK
+    torch.cuda.synchronize()
+    assert lib.lct_device_status(None) in (capi.LCT_OK, capi.LCT_ERR_ARG)
