@@ -18,9 +18,10 @@
 // of two TMEM buffers.  Fused epilogues: bias + ReLU -> bf16 (forward), ReLU mask of the
 // previous activation -> bf16 delta (backward data), FP32 residual (training), and the
 // acceptance gate writing the corrected volume (inference).
-// Weight gradients: SIMT FP32 outer products over row segments staged in shared memory.
+// Weight gradients: the same tcgen05 machinery with K = pixels (both operands MN-major).
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <new>
 #include <vector>
@@ -380,81 +381,149 @@ __global__ void __launch_bounds__(256) cnn_loss_kernel(const float* __restrict__
   }
 }
 
-// Weight / bias gradients of one layer: dW[co][ci][ky][kx] = sum_p dz[p][co] a[p + (ky-1, kx-1)][ci].
-// Segment = 64 pixels of one row; thread (ky, 4 co, 4 ci) keeps 4 x 4 x 3 FP32 partial sums over
-// the CTA's segments and adds them to the gradient once.
-constexpr int kDwSeg = 64, kDwThreads = 192;
-__global__ void __launch_bounds__(kDwThreads) cnn_dw_kernel(const __nv_bfloat16* __restrict__ act,
-                                                            const __nv_bfloat16* __restrict__ dz,
-                                                            int B, int H, int W, int wp, int cin,
-                                                            int cout, float* __restrict__ gw,
-                                                            float* __restrict__ gb) {
-  __shared__ __align__(16) __nv_bfloat16 s_a[3][kDwSeg + 2][kCnnC];
-  __shared__ __align__(16) __nv_bfloat16 s_d[kDwSeg][kCnnC];
-  const int t = threadIdx.x, ky = t / 64, rem = t % 64, cog = rem / 8, cig = rem % 8;
-  float acc[4][4][3];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) acc[i][j][k] = 0.f;
-  float accb[4] = {0.f, 0.f, 0.f, 0.f};
-  const bool bias_thread = ky == 0 && cig == 0;
-  const int segs_x = (W + kDwSeg - 1) / kDwSeg;
-  const long long n_segs = (long long)B * H * segs_x;
-  for (long long sg = blockIdx.x; sg < n_segs; sg += gridDim.x) {
-    const int sx = (int)(sg % segs_x);
-    const long long q = sg / segs_x;
-    const int y = (int)(q % H), b = (int)(q / H), x0 = sx * kDwSeg;
-    __syncthreads();
-    for (int i = t; i < 3 * (kDwSeg + 2) * 4; i += kDwThreads) {
-      const int g = i & 3, px = (i >> 2) % (kDwSeg + 2), r = (i >> 2) / (kDwSeg + 2);
-      const int yy = y + r - 1, col = x0 + px;  // padded column
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (yy >= 0 && yy < H && col < wp)
-        v = reinterpret_cast<const uint4*>(act + (((long long)b * H + yy) * wp + col) * kCnnC)[g];
-      reinterpret_cast<uint4*>(&s_a[r][px][0])[g] = v;
+// Weight gradients of one layer on tcgen05, no transposes: with K = pixels, both channels-last
+// operands are MN-major (32 channels = one 64-byte swizzle row per pixel, 8 pixels = one atom).
+//   D_dx[dy * 32 + ci][co] += sum_p act[p + (dy - 1, dx - 1)][ci] * dz[p][co]
+// Per 8 px x 16 rows tile: one activation box {32 ch, 8 px, 19 rows} per dx whose rows r and
+// r + 1 .. are the dy blocks (M = 128: the three dy blocks at +512 B and one discarded block),
+// and one delta box {32 ch, 8 px, 16 rows} (N = 32); K = 128 pixels = 8 MMAs of K16 per dx.
+// A CTA accumulates over all its tiles in three TMEM accumulators and adds them to the gradient
+// once.  Pads and rows outside the image are zero in the deltas, so they add nothing.
+constexpr int kDwStages = 3, kDwThreads = 128, kDwRows = kConvTH + 3;
+struct DwCfg {
+  static constexpr uint32_t BoxA = kConvTW * kDwRows * kCnnC * 2;  // 9728 B
+  static constexpr uint32_t BoxD = kConvTW * kConvTH * kCnnC * 2;  // 8192 B
+  static constexpr uint32_t Stage = 3 * BoxA + BoxD;               // 37376 B, 512-aligned
+  static constexpr uint32_t Smem = 1024 + kDwStages * Stage + 128;
+  static constexpr uint32_t TmemCols = 128;                         // 3 x 32 used
+  static constexpr uint32_t Idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                                    ((uint32_t)(32 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+};
+
+__global__ void __launch_bounds__(kDwThreads)
+    cnn_dw_tc_kernel(const __grid_constant__ CUtensorMap ma, const __grid_constant__ CUtensorMap mz,
+                     const ConvArgs a, int cin, int cout, float* __restrict__ gw) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kDwStages * DwCfg::Stage);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kDwStages + 1);
+  __shared__ int s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t full0 = smem_u32(&bars[0]);
+  const uint32_t empty0 = smem_u32(&bars[kDwStages]);
+  const uint32_t mdone = smem_u32(&bars[2 * kDwStages]);
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (int s = 0; s < kDwStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
     }
-    for (int i = t; i < kDwSeg * 4; i += kDwThreads) {
-      const int g = i & 3, px = i >> 2, x = x0 + px;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (x < W)
-        v = reinterpret_cast<const uint4*>(dz + (((long long)b * H + y) * wp + x + 1) * kCnnC)[g];
-      reinterpret_cast<uint4*>(&s_d[px][0])[g] = v;
+    mbar_init(mdone, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(DwCfg::TmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    long long it = 0;
+    for (long long t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int s = (int)(it % kDwStages);
+      if (it >= kDwStages &&
+          !mbar_wait(empty0 + 8 * s, (uint32_t)(((it / kDwStages) - 1) & 1))) {
+        atomicExch(&s_abort, 1);
+        break;
+      }
+      if (conv_aborted(&s_abort)) break;
+      int x0, y0, b;
+      conv_tile(a, t, x0, y0, b);
+      uint8_t* st = smem + s * DwCfg::Stage;
+      const uint32_t fb = full0 + 8 * s;
+      mbar_expect_tx(fb, DwCfg::Stage);
+      for (int dx = 0; dx < 3; ++dx)  // pixel x, column offset dx - 1: padded column x + dx
+        tma_load_4d(smem_u32(st + dx * DwCfg::BoxA), &ma, 0, x0 + dx, y0 - 1, b, fb);
+      tma_load_4d(smem_u32(st + 3 * DwCfg::BoxA), &mz, 0, x0 + 1, y0, b, fb);
     }
-    __syncthreads();
-#pragma unroll 4
-    for (int p = 0; p < kDwSeg; ++p) {
-      const uint2 dv = *reinterpret_cast<const uint2*>(&s_d[p][cog * 4]);
-      const float d[4] = {bf16_lo(dv.x), bf16_hi(dv.x), bf16_lo(dv.y), bf16_hi(dv.y)};
-      if (bias_thread)
+    if (conv_aborted(&s_abort))  // let copies in flight land before the CTA exits
+      for (long long k = (it > kDwStages ? it - kDwStages : 0); k < it; ++k)
+        mbar_wait(full0 + 8 * (int)(k % kDwStages), (uint32_t)((k / kDwStages) & 1));
+  } else if (warp == 1 && lane == 0) {
+    long long it = 0;
+    bool first = true;
+    for (long long t = blockIdx.x; t < a.n_tiles; t += gridDim.x, ++it) {
+      const int s = (int)(it % kDwStages);
+      if (!mbar_wait(full0 + 8 * s, (uint32_t)((it / kDwStages) & 1))) {
+        atomicExch(&s_abort, 1);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t st = smem_u32(smem + s * DwCfg::Stage);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) accb[c] += d[c];
+      for (int dx = 0; dx < 3; ++dx) {
 #pragma unroll
-      for (int kx = 0; kx < 3; ++kx) {
-        const uint2 av = *reinterpret_cast<const uint2*>(&s_a[ky][p + kx][cig * 4]);
-        const float v[4] = {bf16_lo(av.x), bf16_hi(av.x), bf16_lo(av.y), bf16_hi(av.y)};
+        for (int k = 0; k < kConvTH / 2; ++k) {  // K16 = two 8-pixel atoms = 1024 B
+          const uint64_t da = desc_mn_sw64(st + dx * DwCfg::BoxA + k * 1024, 512, 512);
+          const uint64_t dz = desc_mn_sw64(st + 3 * DwCfg::BoxA + k * 1024, 512, 512);
+          umma_bf16(tmem + dx * 32, da, dz, DwCfg::Idesc, (first && k == 0) ? 0u : 1u);
+        }
+      }
+      first = false;
+      umma_commit(empty0 + 8 * s);
+    }
+    umma_commit(mdone);
+  }
+  __syncwarp();
+  const bool done = __all_sync(0xFFFFFFFFu, mbar_wait(mdone, 0));
+  __syncthreads();
+  tc_fence_after();
+  if (!done || conv_aborted(&s_abort)) {
+    if (threadIdx.x == 0 && a.status) atomicExch(a.status, kDevWaitTimeout);
+  } else if (blockIdx.x < a.n_tiles) {
+    // warp w holds rows 32 w ..: dy = w (w = 3 is the discarded block), ci = lane
+    const int dy = warp, ci = lane;
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
+    for (int dx = 0; dx < 3; ++dx) {
+      uint32_t r[32];
+      tmem_ld32(tmem + dx * 32 + ((uint32_t)(warp * 32) << 16), r);
+      if (dy < 3 && ci < cin) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[c][j][kx] = fmaf(d[c], v[j], acc[c][j][kx]);
+        for (int co = 0; co < 32; ++co)
+          if (co < cout) atomicAdd(&gw[((co * cin + ci) * 3 + dy) * 3 + dx], __uint_as_float(r[co]));
       }
     }
   }
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int co = cog * 4 + c;
-    if (co >= cout) continue;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int ci = cig * 4 + j;
-      if (ci >= cin) continue;
-#pragma unroll
-      for (int kx = 0; kx < 3; ++kx)
-        atomicAdd(&gw[((co * cin + ci) * 3 + ky) * 3 + kx], acc[c][j][kx]);
-    }
-    if (bias_thread) atomicAdd(&gb[co], accb[c]);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(DwCfg::TmemCols)
+                 : "memory");
+}
+
+// Bias gradients: sum of the deltas over the slices' padded pixels (pads are zero).
+__global__ void __launch_bounds__(256) cnn_db_kernel(const __nv_bfloat16* __restrict__ dz,
+                                                     long long n_pix, int cout,
+                                                     float* __restrict__ gb) {
+  __shared__ float red[8][kCnnC];
+  const int c = threadIdx.x & 31, g = threadIdx.x >> 5;
+  float acc = 0.f;
+  for (long long p = (long long)blockIdx.x * 8 + g; p < n_pix; p += (long long)gridDim.x * 8)
+    acc += __bfloat162float(dz[p * kCnnC + c]);
+  red[g][c] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = 0.f;
+    for (int k = 0; k < 8; ++k) v += red[k][threadIdx.x];
+    if (threadIdx.x < cout) atomicAdd(&gb[threadIdx.x], v);
   }
 }
 
@@ -509,6 +578,7 @@ struct lct_cnn {
   double* d_loss = nullptr;
   unsigned long long* d_rej = nullptr;
   CUtensorMap m_act[kCnnLayers], m_dz[3], m_wf[kCnnLayers], m_wb[kCnnLayers];
+  CUtensorMap m_dwa[kCnnLayers], m_dwz[3];  // weight-gradient boxes
   float calib = 1.f, in_scale = 1.f;
   int adam_t = 0;
   long long last_n = 0;
@@ -521,13 +591,14 @@ static __nv_bfloat16* dz_buf(lct_cnn* c, int i) { return c->d_dz + (size_t)i * c
 // input buffer of layer l (training keeps every activation; inference ping-pongs two)
 static int act_in(const lct_cnn* c, int l) { return c->train ? l : (l & 1); }
 
-static int act_map(CUtensorMap* m, const void* base, int cap, int H, int wp) {
+// channels-last bf16 [cap][H][wp][32], box {32 ch, 8 px, rows, 1 slice}, 64-byte swizzle
+static int act_map(CUtensorMap* m, const void* base, int cap, int H, int wp, int rows) {
   auto fn = tensor_map_encoder();
   if (!fn) return LCT_ERR_UNSUPPORTED;
   cuuint64_t dims[4] = {(cuuint64_t)kCnnC, (cuuint64_t)wp, (cuuint64_t)H, (cuuint64_t)cap};
   cuuint64_t strides[3] = {(cuuint64_t)kCnnC * 2, (cuuint64_t)wp * kCnnC * 2,
                            (cuuint64_t)H * wp * kCnnC * 2};
-  cuuint32_t box[4] = {(cuuint32_t)kCnnC, (cuuint32_t)kConvTW, (cuuint32_t)(kConvTH + 2), 1};
+  cuuint32_t box[4] = {(cuuint32_t)kCnnC, (cuuint32_t)kConvTW, (cuuint32_t)rows, 1};
   cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides,
                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
@@ -551,16 +622,15 @@ static int weight_map(CUtensorMap* m, const void* base, int rows) {
 // per device: dynamic shared memory set, and resident CTAs per SM of each variant
 static bool conv_attr_done[64];
 static int conv_occ[64][2];
+static int dw_occ[64];
 
-template <int N, int EPI>
-static int conv_attr(int* occ) {
-  int st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<N, EPI>,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            ConvCfg<N>::Smem));
+template <typename K>
+static int tc_attr(K kernel, int smem_bytes, int threads, int* occ) {
+  int st = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            smem_bytes));
   // all of the unified L1 as shared memory, so that several CTAs fit on an SM
   if (!st)
-    st = cuda_status(cudaFuncSetAttribute(conv_tc_kernel<N, EPI>,
-                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+    st = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                           cudaSharedmemCarveoutMaxShared));
   // resident CTAs per SM from the kernel's own resources (shared memory, registers, threads);
   // the runtime's occupancy query answers 1 for this kernel although three fit.  CTAs never
@@ -568,15 +638,15 @@ static int conv_attr(int* occ) {
   cudaFuncAttributes fa;
   int dev = 0;
   cudaDeviceProp pr;
-  if (!st) st = cuda_status(cudaFuncGetAttributes(&fa, conv_tc_kernel<N, EPI>));
+  if (!st) st = cuda_status(cudaFuncGetAttributes(&fa, kernel));
   if (!st) st = cuda_status(cudaGetDevice(&dev));
   if (!st) st = cuda_status(cudaGetDeviceProperties(&pr, dev));
   if (st) return st;
-  const size_t smem = ConvCfg<N>::Smem + fa.sharedSizeBytes + pr.reservedSharedMemPerBlock;
+  const size_t smem = smem_bytes + fa.sharedSizeBytes + pr.reservedSharedMemPerBlock;
   const int by_smem = (int)(pr.sharedMemPerMultiprocessor / smem);
   const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
-  const int by_regs = pr.regsPerMultiprocessor / (regs_warp * (kConvThreads / 32));
-  const int by_threads = pr.maxThreadsPerMultiProcessor / kConvThreads;
+  const int by_regs = pr.regsPerMultiprocessor / (regs_warp * (threads / 32));
+  const int by_threads = pr.maxThreadsPerMultiProcessor / threads;
   int o = by_smem < by_regs ? by_smem : by_regs;
   o = o < by_threads ? o : by_threads;
   *occ = o;
@@ -587,10 +657,11 @@ static int conv_prepare(int dev) {
   if (dev < 0 || dev >= 64) return LCT_ERR_UNSUPPORTED;
   if (conv_attr_done[dev]) return LCT_OK;
   int st, o[4];
-  if ((st = conv_attr<32, kEpiRelu>(&o[0]))) return st;
-  if ((st = conv_attr<32, kEpiMask>(&o[1]))) return st;
-  if ((st = conv_attr<16, kEpiResid>(&o[2]))) return st;
-  if ((st = conv_attr<16, kEpiGate>(&o[3]))) return st;
+  if ((st = tc_attr(conv_tc_kernel<32, kEpiRelu>, ConvCfg<32>::Smem, kConvThreads, &o[0]))) return st;
+  if ((st = tc_attr(conv_tc_kernel<32, kEpiMask>, ConvCfg<32>::Smem, kConvThreads, &o[1]))) return st;
+  if ((st = tc_attr(conv_tc_kernel<16, kEpiResid>, ConvCfg<16>::Smem, kConvThreads, &o[2]))) return st;
+  if ((st = tc_attr(conv_tc_kernel<16, kEpiGate>, ConvCfg<16>::Smem, kConvThreads, &o[3]))) return st;
+  if ((st = tc_attr(cnn_dw_tc_kernel, DwCfg::Smem, kDwThreads, &dw_occ[dev]))) return st;
   conv_occ[dev][0] = o[0] < o[1] ? o[0] : o[1];
   conv_occ[dev][1] = o[2] < o[3] ? o[2] : o[3];
   conv_attr_done[dev] = true;
@@ -676,15 +747,21 @@ static int cnn_backward_impl(lct_cnn* c, const float* d_in5, const float* d_targ
       (float)(2.0 / (double)n), dz_buf(c, 2), c->d_loss);
   if ((st = launch_status())) return st;
   c->last_n = n;
-  const long long segs = (long long)B * c->H * ((c->W + kDwSeg - 1) / kDwSeg);
-  const int dw_grid = (int)(segs < (long long)c->sms * 4 ? segs : (long long)c->sms * 4);
   ConvArgs a = conv_args(c);
+  ConvArgs da = conv_args(c);
+  da.n_tiles = (long long)B * da.tiles_x * da.tiles_y;
+  const long long dw_res = (long long)c->sms * dw_occ[c->device];
+  const unsigned dw_grid = (unsigned)(da.n_tiles < dw_res ? da.n_tiles : dw_res);
+  const long long n_pix = (long long)B * c->H * c->wp;
+  const unsigned db_grid = (unsigned)std::min<long long>((n_pix + 7) / 8, (long long)c->sms * 8);
   int cur = 2;
   for (int l = kCnnLayers - 1; l >= 0; --l) {
     float* gw = c->d_g + cnn_off(l);
     float* gb = gw + cnn_cin(l) * cnn_cout(l) * 9;
-    cnn_dw_kernel<<<dw_grid, kDwThreads, 0, s>>>(act_buf(c, l), dz_buf(c, cur), B, c->H, c->W,
-                                                 c->wp, cnn_cin(l), cnn_cout(l), gw, gb);
+    cnn_dw_tc_kernel<<<dw_grid, kDwThreads, DwCfg::Smem, s>>>(c->m_dwa[l], c->m_dwz[cur], da,
+                                                                cnn_cin(l), cnn_cout(l), gw);
+    if ((st = launch_status())) return st;
+    cnn_db_kernel<<<db_grid, 256, 0, s>>>(dz_buf(c, cur), n_pix, cnn_cout(l), gb);
     if ((st = launch_status())) return st;
     if (l == 0) break;
     const int nxt = cur == 2 ? 0 : (cur ^ 1);
@@ -788,9 +865,14 @@ LCT_API int lct_cnn_create(int max_slices, int ny, int nx, int flags, uint64_t s
   }
   if (!st) st = cuda_status(cudaMalloc(&c->d_loss, sizeof(double)));
   if (!st) st = cuda_status(cudaMalloc(&c->d_rej, sizeof(unsigned long long)));
-  for (int i = 0; i < c->n_act && !st; ++i) st = act_map(&c->m_act[i], act_buf(c, i), c->cap, c->H, c->wp);
+  for (int i = 0; i < c->n_act && !st; ++i)
+    st = act_map(&c->m_act[i], act_buf(c, i), c->cap, c->H, c->wp, kConvTH + 2);
   for (int i = 0; i < 3 && !st && c->train; ++i)
-    st = act_map(&c->m_dz[i], dz_buf(c, i), c->cap, c->H, c->wp);
+    st = act_map(&c->m_dz[i], dz_buf(c, i), c->cap, c->H, c->wp, kConvTH + 2);
+  for (int i = 0; i < c->n_act && !st && c->train; ++i)  // weight gradients: 19-row boxes
+    st = act_map(&c->m_dwa[i], act_buf(c, i), c->cap, c->H, c->wp, kDwRows);
+  for (int i = 0; i < 3 && !st && c->train; ++i)
+    st = act_map(&c->m_dwz[i], dz_buf(c, i), c->cap, c->H, c->wp, kConvTH);
   for (int l = 0; l < kCnnLayers && !st; ++l) {
     st = weight_map(&c->m_wf[l], c->d_wf + (size_t)l * kWSlot, l == kCnnLayers - 1 ? 16 : 32);
     if (!st) st = weight_map(&c->m_wb[l], c->d_wb + (size_t)l * kWSlot, 32);

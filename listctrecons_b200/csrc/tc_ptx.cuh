@@ -88,6 +88,17 @@ __device__ __forceinline__ uint64_t desc_sw64(uint32_t addr) {
   d |= (uint64_t)4 << 61;           // 64-byte swizzle
   return d;
 }
+// MN-major operand, 64-byte swizzle: 8-k x 64-byte atoms holding 32 MN elements each; lbo =
+// bytes between 32-element MN blocks, sbo = bytes between 8-k atoms
+__device__ __forceinline__ uint64_t desc_mn_sw64(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version
+  d |= (uint64_t)4 << 61;  // 64-byte swizzle
+  return d;
+}
 __device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc,
                                           uint32_t acc) {
   asm volatile(
