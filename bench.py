@@ -605,7 +605,7 @@ def run_learned(args, rank, world, dist):
         "accuracy_vs_phantom": acc,
         "training": {"ms_per_step": t_ms, "slices_per_step": 16,
                      "tflops": pix * 3 * CNN_FLOP_PER_VOXEL / (t_ms / 1e3) / 1e12,
-                     "note": "forward + backward (tcgen05 data gradients, SIMT weight gradients) + Adam"},
+                     "note": "forward + backward (tcgen05 data and weight gradients) + Adam"},
         "gpu_launches": launches,
         "clocks": clk,
     }

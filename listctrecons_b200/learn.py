@@ -29,8 +29,8 @@ CIN = (5, 32, 32, 32, 32, 32, 32, 32)
 COUT = (32, 32, 32, 32, 32, 32, 32, 1)
 # 1/mm: largest accepted |corrected - plain|.  On the learned configuration plain FDK is off by
 # several mu_water where photons starve (40 overlapping ellipsoids, I0 = 1e5) and at pitch 1.5;
-# a 2 mu_water gate rejects 14% of the voxels and keeps little of the correction, 10 mu_water
-# rejects 0.35% (the benchmark reports the sweep).
+# a 2 mu_water gate rejects about 15% of the voxels and keeps little of the correction, 10 mu_water
+# about 1% (the benchmark reports the sweep).
 DEFAULT_BOUND = 10.0 * MU_WATER
 
 
