@@ -242,13 +242,13 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
           const float fj = (float)j;
           const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
           const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
-          const float r = __fdividef(1.0f, qh1 - qh2);
-          const float in1 = -qh2 * r, in2 = qh1 * r;
+          // the pair weights sum to one in every case -- (-qh2, qh1) / (qh1 - qh2), (0, 1),
+          // (1, 0), (1/2, 1/2) -- so w1 s1 + w2 s2 = s2 + w1 (s1 - s2)
+          const float in1 = -qh2 * __fdividef(1.0f, qh1 - qh2);
           const float w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
-          const float w2 = out2 ? (out1 ? 0.5f : 0.0f) : (out1 ? 1.0f : in2);
           const float s1 = quad_sample_exact(q1, A.qcols, A.nt, a1, fmaf(fj, kd1, u1));
           const float s2 = quad_sample_exact(q2, A.qcols, A.nt, a2, fmaf(fj, kd2, u2));
-          acc[j] = fmaf(w1, s1, fmaf(w2, s2, acc[j]));
+          acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
         };
         if (jlo == 0 && jhi == NZ) {
 #pragma unroll
