@@ -748,7 +748,10 @@ def run_ours(args, rank, world, dist):
         "roofline": {"kernel": "bp_quad_kernel", "bound": "hbm", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
-                     "algorithmic_bytes": alg_bytes, "launch_ms": bp},
+                     "algorithmic_bytes": alg_bytes, "launch_ms": bp,
+                     "note": "each filtered view is reused ~150x from L1/L2, so HBM is not this "
+                             "kernel's bound: it is issue-bound (79% of issue slots, ncu) -- see "
+                             "roofline_onchip and profiles/bp_quad_kernel_*.md"},
         "roofline_onchip": {"bound": "l1", "achieved": l1_achieved, "peak": l1_peak, "unit": "GB/s",
                             "frac": l1_achieved / l1_peak,
                             "note": "32 B per voxel-view update (8 FP32 taps) vs 128 B/clk/SM nominal "
