@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -655,6 +656,8 @@ static int tc_attr(K kernel, int smem_bytes, int threads, int* occ) {
 
 static int conv_prepare(int dev) {
   if (dev < 0 || dev >= 64) return LCT_ERR_UNSUPPORTED;
+  static std::mutex mu;  // host threads may create workspaces on one device together
+  std::lock_guard<std::mutex> lock(mu);
   if (conv_attr_done[dev]) return LCT_OK;
   int st, o[4];
   if ((st = tc_attr(conv_tc_kernel<32, kEpiRelu>, ConvCfg<32>::Smem, kConvThreads, &o[0]))) return st;

@@ -306,12 +306,16 @@ static int tc_filter_p(int ns, float* d_rows, long long nrows, void* scratch, cu
   }
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 64 && !tc_attr_done[P - 2][dev]) {
-    if ((st = cuda_status(cudaFuncSetAttribute(filter_tc_kernel<P>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               Cfg::Smem))))
-      return st;
-    tc_attr_done[P - 2][dev] = true;
+  {
+    static std::mutex mu;  // host threads may share a device
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 64 || !tc_attr_done[P - 2][dev]) {
+      if ((st = cuda_status(cudaFuncSetAttribute(filter_tc_kernel<P>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 Cfg::Smem))))
+        return st;
+      if (dev < 64) tc_attr_done[P - 2][dev] = true;
+    }
   }
   dim3 grid(kp / Cfg::N, (unsigned)mt);
   filter_tc_kernel<P><<<grid, kTcThreads, Cfg::Smem, s>>>(maps, d_rows, nrows, ns, kp / kTcK,
