@@ -274,7 +274,8 @@ def run_batch(args, rank, world, dist):
         "stages_ms": {k: statistics.mean(t[k] for t in stage) for k in stage[0]},
         "e2e": {"value": upd / (e2e_ms / 1e3) / 1e9, "unit": UNIT, "s_per_batch": e2e_ms / 1e3,
                 "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
-        "gpu_launches_note": "per step: 3 graph launches (rebin, filter, one persistent BP)",
+        "gpu_launches_note": "per step: 3 graph launches (rebin, filter, backprojection: one "
+                             "persistent work list per thread shape)",
     }
     print(json.dumps(line), flush=True)
     return 0

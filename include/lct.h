@@ -335,7 +335,8 @@ int lct_cnn_param_count(int64_t* n);
 /* Workspace for up to max_slices slices of ny x nx; weights He-initialised from seed.
    Synchronous. */
 int lct_cnn_create(int max_slices, int ny, int nx, int flags, uint64_t seed, lct_cnn** out);
-/* Parameter copies (host or device pointers, synchronous).  set_params resets the Adam state. */
+/* Parameter copies (host or device pointers; synchronous: they wait for all work on the device
+   first).  set_params resets the Adam state. */
 int lct_cnn_set_params(lct_cnn* c, const float* params, int on_device);
 int lct_cnn_get_params(const lct_cnn* c, float* params, int on_device);
 int lct_cnn_get_grads(const lct_cnn* c, float* grads, int on_device);
@@ -355,7 +356,7 @@ int lct_cnn_adam_step(lct_cnn* c, float lr, float beta1, float beta2, float eps,
                       lct_stream stream);
 int lct_cnn_train_step(lct_cnn* c, const float* d_in5, const float* d_target, int n_slices,
                        float lr, lct_stream stream);
-/* loss of the last backward pass (synchronous) */
+/* loss of the last backward pass (synchronous: waits for all work on the device) */
 int lct_cnn_last_loss(const lct_cnn* c, double* loss);
 /* Inference with the acceptance gate over a device volume d_vol [nz][ny][nx] (raw FDK) ->
    d_out (corrected, phantom units; must not alias d_vol), max_slices slices per pass, edge
@@ -363,7 +364,7 @@ int lct_cnn_last_loss(const lct_cnn* c, double* loss);
    value; when given, the call synchronises the stream. */
 int lct_cnn_infer_volume(lct_cnn* c, const float* d_vol, float* d_out, int nz, float bound,
                          int64_t* n_rejected, lct_stream stream);
-/* rejected-voxel count of the last infer_volume (synchronous; call after its stream finished) */
+/* rejected-voxel count of the last infer_volume (synchronous: waits for all work on the device) */
 int lct_cnn_last_rejected(const lct_cnn* c, int64_t* n);
 int lct_cnn_get_shape(const lct_cnn* c, int* max_slices, int* ny, int* nx);
 void lct_cnn_destroy(lct_cnn* c);

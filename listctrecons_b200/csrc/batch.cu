@@ -1,25 +1,35 @@
 // Batched reconstruction of many independent helical scans (uneven length, pitch, rows, columns,
 // volume): every buffer is owned per scan (one lct_recon each, allocated once), and a run is
 //   upload fans -> [graph] rebin all scans -> [graph] filter + quad pack all scans
-//               -> [graph] ONE persistent work-list backprojection over every scan's tiles
+//               -> [graph] persistent work-list backprojection over every scan's tiles (one
+//                  launch per thread shape: each scan keeps the shape its own run would use)
 //               -> download volumes.
 // The three stage graphs are captured once at create (after one eager warm-up run, which also
 // sets kernel attributes and loads modules).  The work-list kernel balances the uneven scans
 // across the SMs; each tile runs the arithmetic of its scan's own launch, so a scan's volume is
 // bit-identical to lct_recon_run with the same options.
+#include <map>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "recon_internal.h"
 
+// One work list per backprojection thread shape: the scans that share a shape (slices per
+// thread, CTAs per SM) run in one persistent launch.
+struct BpGroup {
+  int nz = 8, minb = 4, n = 0;
+  void* d_args = nullptr;    // per-scan backprojection arguments
+  int* d_prefix = nullptr;   // tile prefix sums, n + 1
+  int* d_counter = nullptr;  // work-list cursor, zeroed by the graph before each launch
+};
+
 struct lct_batch {
   std::vector<lct_recon*> recs;
   cudaGraphExec_t exec[3] = {};
-  void* d_args = nullptr;    // per-scan backprojection arguments (work list)
-  int* d_prefix = nullptr;   // tile prefix sums, n_scans + 1
-  int* d_counter = nullptr;  // work-list cursor, zeroed by the graph before each launch
+  std::vector<BpGroup> groups;
   bool worklist = false;
-  int nz = 8, minb = 4, interp = LCT_INTERP_TEX8;
+  int interp = LCT_INTERP_TEX8;
   cudaEvent_t ev[6] = {};
   float times[5] = {};
   int launches = 0;
@@ -32,9 +42,11 @@ static void free_batch(lct_batch* b) {
   for (auto& e : b->exec)
     if (e) cudaGraphExecDestroy(e);
   for (auto* r : b->recs) lct_recon_destroy(r);
-  cudaFree(b->d_args);
-  cudaFree(b->d_prefix);
-  cudaFree(b->d_counter);
+  for (auto& gr : b->groups) {
+    cudaFree(gr.d_args);
+    cudaFree(gr.d_prefix);
+    cudaFree(gr.d_counter);
+  }
   for (auto& e : b->ev)
     if (e) cudaEventDestroy(e);
   delete b;
@@ -43,9 +55,13 @@ static void free_batch(lct_batch* b) {
 static int batch_stage(lct_batch* b, int stage, cudaStream_t s) {
   int st = LCT_OK;
   if (stage == 2 && b->worklist) {
-    if ((st = cuda_status(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s)))) return st;
-    return launch_bp_quad_worklist(b->d_args, b->d_prefix, (int)b->recs.size(), b->d_counter,
-                                   b->nz, b->interp, b->minb, s);
+    for (auto& gr : b->groups) {
+      if ((st = cuda_status(cudaMemsetAsync(gr.d_counter, 0, sizeof(int), s)))) return st;
+      if ((st = launch_bp_quad_worklist(gr.d_args, gr.d_prefix, gr.n, gr.d_counter, gr.nz,
+                                        b->interp, gr.minb, s)))
+        return st;
+    }
+    return LCT_OK;
   }
   for (auto* r : b->recs) {
     if (stage == 0)
@@ -105,33 +121,46 @@ LCT_API int lct_batch_create(const lct_plan* const* plans, int n, const lct_reco
       if (!recon_bp_quads_all(r) || r->o.interp != b->interp) b->worklist = false;
   }
   if (!st && b->worklist) {
+    // each scan keeps the thread shape its own run would use (the slices-per-thread heuristic,
+    // or the requested / autotuned shape); scans sharing a shape share a work list
     const int asz = bp_quad_args_size();
-    std::vector<char> args((size_t)asz * n);
-    std::vector<int> prefix(n + 1, 0);
-    for (int i = 0; i < n && !st; ++i) {
+    std::map<std::pair<int, int>, std::vector<int>> by_shape;
+    for (int i = 0; i < n; ++i) {
       lct_recon* r = b->recs[i];
       BpLaunch L;
       recon_bp_launch(r, 0, r->info.n_blocks_run, r->d_img, L);
-      if (i == 0) {
-        b->nz = L.nz_thread;
-        b->minb = L.minb > 0 ? L.minb : 4;
-      }
-      L.nz_thread = b->nz;
-      L.minb = b->minb;
-      r->o.bp_nz = b->nz;  // the scans' own launches use the same thread shape
-      r->o.bp_minb = b->minb;
-      int tiles = 0;
-      st = bp_quad_args_build(r->info.ctg, r->info.ig, L, r->d_quad, args.data() + (size_t)asz * i,
-                              &tiles);
-      prefix[i + 1] = prefix[i] + tiles;
+      r->o.bp_nz = L.nz_thread;  // the scan's own launches use the same shape
+      r->o.bp_minb = L.minb > 0 ? L.minb : 4;
+      by_shape[{r->o.bp_nz, r->o.bp_minb}].push_back(i);
     }
-    if (!st) st = cuda_status(cudaMalloc(&b->d_args, args.size()));
-    if (!st) st = cuda_status(cudaMalloc(&b->d_prefix, sizeof(int) * (n + 1)));
-    if (!st) st = cuda_status(cudaMalloc(&b->d_counter, sizeof(int)));
-    if (!st) st = cuda_status(cudaMemcpy(b->d_args, args.data(), args.size(), cudaMemcpyHostToDevice));
-    if (!st)
-      st = cuda_status(cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int) * (n + 1),
-                                  cudaMemcpyHostToDevice));
+    for (auto& kv : by_shape) {
+      if (st) break;
+      BpGroup gr;
+      gr.nz = kv.first.first;
+      gr.minb = kv.first.second;
+      gr.n = (int)kv.second.size();
+      std::vector<char> args((size_t)asz * gr.n);
+      std::vector<int> prefix(gr.n + 1, 0);
+      for (int k = 0; k < gr.n && !st; ++k) {
+        lct_recon* r = b->recs[kv.second[k]];
+        BpLaunch L;
+        recon_bp_launch(r, 0, r->info.n_blocks_run, r->d_img, L);
+        int tiles = 0;
+        st = bp_quad_args_build(r->info.ctg, r->info.ig, L, r->d_quad,
+                                args.data() + (size_t)asz * k, &tiles);
+        prefix[k + 1] = prefix[k] + tiles;
+      }
+      b->groups.push_back(gr);
+      BpGroup& g = b->groups.back();
+      if (!st) st = cuda_status(cudaMalloc(&g.d_args, args.size()));
+      if (!st) st = cuda_status(cudaMalloc(&g.d_prefix, sizeof(int) * (gr.n + 1)));
+      if (!st) st = cuda_status(cudaMalloc(&g.d_counter, sizeof(int)));
+      if (!st)
+        st = cuda_status(cudaMemcpy(g.d_args, args.data(), args.size(), cudaMemcpyHostToDevice));
+      if (!st)
+        st = cuda_status(cudaMemcpy(g.d_prefix, prefix.data(), sizeof(int) * (gr.n + 1),
+                                    cudaMemcpyHostToDevice));
+    }
   }
   // eager warm-up on zeroed fans, then capture one graph per stage
   for (auto* r : b->recs)

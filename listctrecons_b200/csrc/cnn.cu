@@ -895,9 +895,13 @@ LCT_API int lct_cnn_create(int max_slices, int ny, int nx, int flags, uint64_t s
   return LCT_OK;
 }
 
+// Parameter, gradient, loss and counter copies wait for every stream first: the caller's training
+// or inference may be queued on a non-blocking stream that the default stream does not order.
 LCT_API int lct_cnn_set_params(lct_cnn* c, const float* params, int on_device) {
   if (!c || !params) return LCT_ERR_ARG;
-  int st = cuda_status(cudaMemcpy(c->d_p, params, sizeof(float) * kCnnParams,
+  int st = cuda_status(cudaDeviceSynchronize());
+  if (st) return st;
+  st = cuda_status(cudaMemcpy(c->d_p, params, sizeof(float) * kCnnParams,
                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
   if (!st) st = cuda_status(cudaMemset(c->d_m, 0, sizeof(float) * 2 * kCnnParams));
   c->adam_t = 0;
@@ -908,12 +912,16 @@ LCT_API int lct_cnn_set_params(lct_cnn* c, const float* params, int on_device) {
 
 LCT_API int lct_cnn_get_params(const lct_cnn* c, float* params, int on_device) {
   if (!c || !params) return LCT_ERR_ARG;
+  const int st = cuda_status(cudaDeviceSynchronize());
+  if (st) return st;
   return cuda_status(cudaMemcpy(params, c->d_p, sizeof(float) * kCnnParams,
                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
 }
 
 LCT_API int lct_cnn_get_grads(const lct_cnn* c, float* grads, int on_device) {
   if (!c || !grads || !c->train) return LCT_ERR_ARG;
+  const int st = cuda_status(cudaDeviceSynchronize());
+  if (st) return st;
   return cuda_status(cudaMemcpy(grads, c->d_g, sizeof(float) * kCnnParams,
                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
 }
@@ -976,7 +984,8 @@ LCT_API int lct_cnn_last_loss(const lct_cnn* c, double* loss) {
   if (!c || !loss || !c->train) return LCT_ERR_ARG;
   if (c->last_n <= 0) return LCT_ERR_ARG;  // no backward pass yet
   double sum = 0.0;
-  int st = cuda_status(cudaMemcpy(&sum, c->d_loss, sizeof(double), cudaMemcpyDeviceToHost));
+  int st = cuda_status(cudaDeviceSynchronize());
+  if (!st) st = cuda_status(cudaMemcpy(&sum, c->d_loss, sizeof(double), cudaMemcpyDeviceToHost));
   if (!st) *loss = sum / (double)c->last_n;
   return st;
 }
@@ -1044,7 +1053,8 @@ LCT_API int lct_cnn_get_shape(const lct_cnn* c, int* max_slices, int* ny, int* n
 LCT_API int lct_cnn_last_rejected(const lct_cnn* c, int64_t* n) {
   if (!c || !n) return LCT_ERR_ARG;
   unsigned long long v = 0;
-  int st = cuda_status(cudaMemcpy(&v, c->d_rej, sizeof(v), cudaMemcpyDeviceToHost));
+  int st = cuda_status(cudaDeviceSynchronize());
+  if (!st) st = cuda_status(cudaMemcpy(&v, c->d_rej, sizeof(v), cudaMemcpyDeviceToHost));
   if (!st) *n = (int64_t)v;
   return st;
 }

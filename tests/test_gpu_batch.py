@@ -1,7 +1,8 @@
 """Batched reconstruction (lct_batch: one graph launch per stage, one persistent work-list
 backprojection over every scan) and the backprojection autotuner.  Bar: each scan's batch volume
-is bit-identical to its own lct_recon run with the same options; the autotuned run equals the
-default one (the thread shape does not change any voxel's arithmetic)."""
+is bit-identical to its own lct_recon run with the same options -- with one requested thread
+shape, and with each scan's own default shape (several work lists); the autotuned run equals the
+default one in TEX8 mode, whose arithmetic per slice does not depend on the thread shape."""
 import numpy as np
 import pytest
 
@@ -34,16 +35,20 @@ def scans(cuda):
     return out
 
 
-@pytest.mark.parametrize("interp", [capi.INTERP_EXACT, capi.INTERP_TEX8])
-def test_batch_equals_single_scan_runs(scans, interp):
+@pytest.mark.parametrize("interp,bp_nz", [(capi.INTERP_EXACT, 8), (capi.INTERP_TEX8, 8),
+                                          (capi.INTERP_EXACT, 0)])
+def test_batch_equals_single_scan_runs(scans, interp, bp_nz):
+    """bp_nz 0: each scan keeps its default shape (4 or 8 slices per thread for these three
+    scans), so the backprojection graph holds one work list per shape."""
     import torch
 
     plans = [p for _, p, _ in scans]
-    b = Batch(plans, interp=interp, filter_mode=capi.FILTER_BF16X6, bp_nz=8)
+    b = Batch(plans, interp=interp, filter_mode=capi.FILTER_BF16X6, bp_nz=bp_nz)
     imgs = b.run([f for _, _, f in scans])
     torch.cuda.synchronize()
     for (geo, p, fan), img in zip(scans, imgs):
-        single = Reconstruction(p, interp=interp, filter_mode=capi.FILTER_BF16X6, bp_nz=8).run(fan)
+        single = Reconstruction(p, interp=interp, filter_mode=capi.FILTER_BF16X6,
+                                bp_nz=bp_nz).run(fan)
         assert torch.equal(img, single)
     # host buffers in and out give the same volumes
     hf = [f.cpu().pin_memory() for _, _, f in scans]
