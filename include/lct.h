@@ -290,7 +290,9 @@ typedef struct lct_batch lct_batch;
 int lct_batch_create(const lct_plan* const* plans, int n_scans, const lct_recon_opts* opts,
                      lct_batch** out);
 /* fans[i]: scan i's views from fan_view0[i] on (host or device, as fan_on_device says);
-   images[i]: [n_blocks_run_i*32][ny][nx].  Synchronous. */
+   images[i]: [n_blocks_run_i*32][ny][nx].  Synchronous.  Host fans stream: the scans' uploads,
+   per-slab compute and downloads overlap on internal streams (same kernels per scan as the
+   device-resident graphs, bit-identical volumes; last_times reports one span). */
 int lct_batch_run(lct_batch* b, const float* const* fans, const int64_t* fan_view0,
                   int fan_on_device, float* const* images, int image_on_device, lct_stream stream);
 /* Per-scan fan range and totals over the batch (voxel_updates, bytes, launches = graph and

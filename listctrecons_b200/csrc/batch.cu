@@ -33,6 +33,8 @@ struct lct_batch {
   cudaEvent_t ev[6] = {};
   float times[5] = {};
   int launches = 0;
+  lct::StreamSet ss;              // streamed runs from host fans (created on first use)
+  std::vector<cudaEvent_t> sev;   // their fork / join events
 };
 
 namespace lct {
@@ -49,6 +51,9 @@ static void free_batch(lct_batch* b) {
   }
   for (auto& e : b->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : b->sev)
+    if (e) cudaEventDestroy(e);
+  streams_destroy(b->ss);
   delete b;
 }
 
@@ -187,6 +192,39 @@ LCT_API int lct_batch_create(const lct_plan* const* plans, int n, const lct_reco
   return LCT_OK;
 }
 
+// Host fans: every scan's streamed run (recon_run_streamed) back to back on shared streams --
+// one upload stream (the scans arrive in order), one download stream, two backprojection
+// streams -- forked once and joined once, so a scan's uploads, rebin and filter overlap the
+// previous scans' backprojections.  Same kernels per scan as the graphs: bit-identical volumes.
+static int batch_run_streamed(lct_batch* b, const float* const* fans, const int64_t* fan_view0,
+                              float* const* images, int image_on_device, cudaStream_t s) {
+  int st = streams_create(b->ss);
+  while (!st && b->sev.size() < 5) {
+    cudaEvent_t e;
+    st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (!st) b->sev.push_back(e);
+  }
+  for (int i = 1; i < 4 && !st; ++i) st = cuda_status(cudaEventRecord(b->ev[i], s));
+  if (!st) st = streams_fork(b->ss, s, b->sev[0]);
+  for (size_t i = 0; i < b->recs.size() && !st; ++i) {
+    lct_recon* r = b->recs[i];
+    if (!fans[i] || !images[i]) return LCT_ERR_ARG;
+    const long long skip = r->fan_first + r->info.data_offset - fan_view0[i];
+    if (skip < 0) return LCT_ERR_ARG;
+    float* d_out = image_on_device ? images[i] : r->d_img;
+    r->launches = 0;
+    st = recon_run_streamed(r, fans[i], skip, d_out, d_out, image_on_device ? nullptr : images[i],
+                            s, b->ss);
+    b->launches += r->launches;
+  }
+  if (!st) st = streams_join(b->ss, s, b->sev.data() + 1);
+  if (!st) st = cuda_status(cudaEventRecord(b->ev[4], s));
+  if (!st) st = cuda_status(cudaEventRecord(b->ev[5], s));
+  if (!st) st = cuda_status(cudaEventSynchronize(b->ev[5]));
+  for (int i = 0; i < 5 && !st; ++i) cudaEventElapsedTime(&b->times[i], b->ev[i], b->ev[i + 1]);
+  return st;
+}
+
 LCT_API int lct_batch_run(lct_batch* b, const float* const* fans, const int64_t* fan_view0,
                           int fan_on_device, float* const* images, int image_on_device,
                           lct_stream stream) {
@@ -195,6 +233,9 @@ LCT_API int lct_batch_run(lct_batch* b, const float* const* fans, const int64_t*
   int st;
   b->launches = 0;
   if ((st = cuda_status(cudaEventRecord(b->ev[0], s)))) return st;
+  bool streamed = !fan_on_device;
+  for (auto* r : b->recs) streamed = streamed && recon_streamable(r) && !r->cnn;
+  if (streamed) return batch_run_streamed(b, fans, fan_view0, images, image_on_device, s);
   const cudaMemcpyKind up = fan_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   for (size_t i = 0; i < b->recs.size(); ++i) {
     lct_recon* r = b->recs[i];

@@ -46,8 +46,7 @@ static void free_recon(lct_recon* r) {
     if (e) cudaEventDestroy(e);
   for (auto& e : r->sev)
     if (e) cudaEventDestroy(e);
-  for (cudaStream_t x : {r->s_up, r->s_down, r->s_bp[0], r->s_bp[1], r->s_cnn})
-    if (x) cudaStreamDestroy(x);
+  streams_destroy(r->ss);
   delete r;
 }
 
@@ -475,26 +474,60 @@ int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s) {
 // on either side are backprojected -- is downloaded on a second copy stream.  Every view is
 // uploaded, rebinned and filtered once by the same kernels as the unstreamed run, so the volume
 // is bit-identical to it.
-static bool streamable(const lct_recon* r) {
+namespace lct {
+
+int streams_create(StreamSet& ss) {
+  cudaStream_t* all[5] = {&ss.up, &ss.down, &ss.bp[0], &ss.bp[1], &ss.cnn};
+  for (auto* a : all) {
+    if (*a) continue;
+    const int st = cuda_status(cudaStreamCreateWithFlags(a, cudaStreamNonBlocking));
+    if (st) return st;
+  }
+  return LCT_OK;
+}
+
+void streams_destroy(StreamSet& ss) {
+  for (cudaStream_t* a : {&ss.up, &ss.down, &ss.bp[0], &ss.bp[1], &ss.cnn})
+    if (*a) {
+      cudaStreamDestroy(*a);
+      *a = nullptr;
+    }
+}
+
+int streams_fork(const StreamSet& ss, cudaStream_t s, cudaEvent_t ev) {
+  int st = cuda_status(cudaEventRecord(ev, s));
+  for (cudaStream_t x : {ss.up, ss.down, ss.bp[0], ss.bp[1], ss.cnn})
+    if (!st) st = cuda_status(cudaStreamWaitEvent(x, ev, 0));
+  return st;
+}
+
+int streams_join(const StreamSet& ss, cudaStream_t s, const cudaEvent_t* ev4) {
+  const cudaStream_t x[4] = {ss.down, ss.bp[0], ss.bp[1], ss.cnn};  // uploads end in s already
+  int st = LCT_OK;
+  for (int i = 0; i < 4 && !st; ++i) {
+    st = cuda_status(cudaEventRecord(ev4[i], x[i]));
+    if (!st) st = cuda_status(cudaStreamWaitEvent(s, ev4[i], 0));
+  }
+  return st;
+}
+
+bool recon_streamable(const lct_recon* r) {
   return r->o.mode == LCT_MODE_SCAN && r->o.rebinner == LCT_REBIN_FAN2PAR &&
          r->o.preweight == LCT_PW_NONE && r->o.backprojector == LCT_BP_PAR;
 }
 
 constexpr long long kStreamPiece = 512;  // global views per upload / rebin / filter piece
 
-static int run_streaming(lct_recon* r, const float* fan_host, long long skip, float* d_img,
-                         float* d_out, float* image_host, cudaStream_t s) {
+int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, float* d_img,
+                       float* d_out, float* image_host, cudaStream_t s, const StreamSet& ss) {
   const lct_geom& g = r->info.ctg;
   const lct_img& ig = r->info.ig;
   const int nb = r->info.n_blocks_run;
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
   const long long plane = r->plane;
   int st;
-  cudaStream_t* aux[5] = {&r->s_up, &r->s_down, &r->s_bp[0], &r->s_bp[1], &r->s_cnn};
-  for (auto* a : aux)
-    if (!*a && (st = cuda_status(cudaStreamCreateWithFlags(a, cudaStreamNonBlocking)))) return st;
-  // events: start, 4 stream ends, per slab: views ready, backprojected, corrected; per piece:
-  // uploaded, packed
+  // events: 5 for the caller's fork and join, per slab: views ready, backprojected, corrected;
+  // per piece: uploaded, packed
   const long long n_pieces = r->g_count / kStreamPiece + nb + 1;
   const size_t n_ev = 5 + 3 * (size_t)nb + 2 * (size_t)n_pieces;
   while (r->sev.size() < n_ev) {
@@ -502,18 +535,12 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
     if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return st;
     r->sev.push_back(e);
   }
-  cudaEvent_t ev_start = r->sev[0];
-  cudaEvent_t* ev_end = r->sev.data() + 1;
-  cudaEvent_t* ev_views = ev_end + 4;
+  cudaEvent_t* ev_views = r->sev.data() + 5;
   cudaEvent_t* ev_bp = ev_views + nb;
   cudaEvent_t* ev_cnn = ev_bp + nb;
   cudaEvent_t* ev_up = ev_cnn + nb;
   cudaEvent_t* ev_packed = ev_up + n_pieces;
   long long piece = 0;
-  // the other streams start after everything already queued on s (an earlier run included)
-  if ((st = cuda_status(cudaEventRecord(ev_start, s)))) return st;
-  for (int i = 0; i < 5; ++i)
-    if ((st = cuda_status(cudaStreamWaitEvent(*aux[i], ev_start, 0)))) return st;
 
   // fan views a range of global views reads (the scan rebin's column shifts, in FP64)
   const double smax = (((double)(g.ns - 1) - (double)g.ws) * (double)g.ds / (double)g.dso) /
@@ -533,10 +560,10 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
   std::vector<char> bp_done(nb, 0), cnn_done(nb, 0);
   auto download = [&](int b, const float* src, cudaEvent_t after) -> int {
     if (!image_host) return LCT_OK;
-    int e = cuda_status(cudaStreamWaitEvent(r->s_down, after, 0));
+    int e = cuda_status(cudaStreamWaitEvent(ss.down, after, 0));
     if (!e)
       e = cuda_status(cudaMemcpyAsync(image_host + b * slab, src + b * slab, sizeof(float) * slab,
-                                      cudaMemcpyDeviceToHost, r->s_down));
+                                      cudaMemcpyDeviceToHost, ss.down));
     return e;
   };
   auto bp = [&](int b, int lo, int hi, int part, cudaStream_t sb) -> int {
@@ -553,7 +580,7 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
   };
   for (int k = 0; k < nb; ++k) {
     const int b = order[k];
-    cudaStream_t sb = r->s_bp[k & 1];
+    cudaStream_t sb = ss.bp[k & 1];
     // the first slab is backprojected in parts as its views arrive (the others' windows are
     // complete by the time their turn comes); only the quad kernel carries parts
     const bool split = k == 0 && r->quads && block_addr(r, b) == packed;
@@ -566,11 +593,11 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
       if (need > up) {
         if ((st = cuda_status(cudaMemcpyAsync(r->d_fan + up * plane, fan_host + (skip + up) * plane,
                                               sizeof(float) * (need - up) * plane,
-                                              cudaMemcpyHostToDevice, r->s_up))))
+                                              cudaMemcpyHostToDevice, ss.up))))
           return st;
         up = need;
       }
-      if ((st = cuda_status(cudaEventRecord(ev_up[piece], r->s_up)))) return st;
+      if ((st = cuda_status(cudaEventRecord(ev_up[piece], ss.up)))) return st;
       if ((st = cuda_status(cudaStreamWaitEvent(s, ev_up[piece], 0)))) return st;
       const long long v0 = done - r->g_first, nv = target - done;
       float* par = r->d_par + v0 * plane;
@@ -621,23 +648,20 @@ static int run_streaming(lct_recon* r, const float* fan_host, long long skip, fl
       if (cnn_done[c] || !bp_done[c] || (c > 0 && !bp_done[c - 1]) || (c + 1 < nb && !bp_done[c + 1]))
         continue;
       for (int n = std::max(0, c - 1); n <= std::min(nb - 1, c + 1); ++n)
-        if ((st = cuda_status(cudaStreamWaitEvent(r->s_cnn, ev_bp[n], 0)))) return st;
+        if ((st = cuda_status(cudaStreamWaitEvent(ss.cnn, ev_bp[n], 0)))) return st;
       if ((st = cnn_infer_range(r->cnn, d_img, d_out, nb * kBlockSlices, c * kBlockSlices,
-                                (c + 1) * kBlockSlices, r->cnn_bound, r->s_cnn)))
+                                (c + 1) * kBlockSlices, r->cnn_bound, ss.cnn)))
         return st;
       r->launches += 9 * cnn_passes(r->cnn, kBlockSlices);
       cnn_done[c] = 1;
-      if ((st = cuda_status(cudaEventRecord(ev_cnn[c], r->s_cnn)))) return st;
+      if ((st = cuda_status(cudaEventRecord(ev_cnn[c], ss.cnn)))) return st;
       if ((st = download(c, d_out, ev_cnn[c]))) return st;
     }
   }
-  // s ends after every other stream
-  for (int i = 1; i < 5; ++i) {
-    if ((st = cuda_status(cudaEventRecord(ev_end[i - 1], *aux[i])))) return st;
-    if ((st = cuda_status(cudaStreamWaitEvent(s, ev_end[i - 1], 0)))) return st;
-  }
   return LCT_OK;
 }
+
+}  // namespace lct
 
 LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                           float* image, int image_on_device, lct_stream stream) {
@@ -655,7 +679,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
   // fan views needed by the run (the union of the blocks' windows)
   const float* d_fan;
   const long long skip = r->fan_first + off - fan_view0;  // views before the run's first
-  if (!fan_on_device && streamable(r)) {
+  if (!fan_on_device && recon_streamable(r)) {
     // host fan: copies overlapped with the compute; one span reported as backprojection
     float* d_out = image_on_device ? image : r->d_img;
     float* d_img = r->cnn ? r->d_plain : d_out;
@@ -663,8 +687,18 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     if (r->cnn && (st = cnn_reset_rejects(r->cnn, s))) return st;
     for (int i = 1; i < 4; ++i)
       if ((st = cuda_status(cudaEventRecord(r->ev[i], s)))) return st;
-    if ((st = run_streaming(r, fan + 0, skip, d_img, d_out, image_on_device ? nullptr : image, s)))
+    if ((st = streams_create(r->ss))) return st;
+    while (r->sev.size() < 5) {
+      cudaEvent_t e;
+      if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return st;
+      r->sev.push_back(e);
+    }
+    // the other streams start after everything already queued on s (an earlier run included)
+    if ((st = streams_fork(r->ss, s, r->sev[0]))) return st;
+    if ((st = recon_run_streamed(r, fan, skip, d_img, d_out, image_on_device ? nullptr : image, s,
+                                 r->ss)))
       return st;
+    if ((st = streams_join(r->ss, s, r->sev.data() + 1))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[5], s)))) return st;
     if ((st = cuda_status(cudaEventSynchronize(r->ev[5])))) return st;
