@@ -45,6 +45,8 @@ struct BpQuadArgs {
   int zchunks;
   int gx, gy, gz;  // tile grid (work-list decoding)
   int view_lo, view_hi, part;  // BpLaunch::view_lo / view_hi / part
+  float kqdz;           // kq * dz (EXACT: row step per slice = kqdz / l)
+  unsigned qrow_bytes;  // bytes per quad row, 16 * qcols
   int slab_view[kBpMaxSlabs];
   int slab_z0[kBpMaxSlabs];
   int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
@@ -113,14 +115,40 @@ __device__ __forceinline__ float quad_sample(const float4* __restrict__ qb, int 
   return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
 }
 
-// EXACT sample: u = row coordinate + 2 (texel centres at integers), so floor(u) is the quad row
-__device__ __forceinline__ float quad_sample_exact(const float4* __restrict__ qb, int qcols,
+// EXACT floor without conversions: for |x| < 2^22, x + 1.5 * 2^23 rounded toward -inf is
+// 1.5 * 2^23 + floor(x) exactly, so its bit pattern is kMagicBits + floor(x) and subtracting the
+// constant back (exact: both operands lie within a factor of two) gives floor(x).  Outside that
+// range the bit pattern still orders like x, so a clamp on it clamps floor(x).
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr int kMagicBits = 0x4B400000;
+
+// view base biased so that a column bit pattern (clamped to kMagicBits + [-2, ns]) times 16 and a
+// row bit pattern (clamped to kMagicBits + [0, nt + 2]) times the row pitch add up to the quad's
+// address: one wide multiply-add per sample
+__device__ __forceinline__ unsigned long long quad_view_bias(const float4* view, unsigned qrow_bytes) {
+  return reinterpret_cast<unsigned long long>(view) - (unsigned long long)(kMagicBits - 2) * 16ull -
+         (unsigned long long)kMagicBits * qrow_bytes;
+}
+
+// EXACT sample: u = row coordinate + 2 (texel centres at integers), so floor(u) is the quad row;
+// col = quad_view_bias(view) + 16 * (column bit pattern)
+__device__ __forceinline__ float quad_sample_exact(unsigned long long col, unsigned qrow_bytes,
                                                    int nt, float a, float u) {
-  const float fu = floorf(u);
-  const float b = u - fu;
-  const int j2 = min(max((int)fu, 0), nt + 2);
-  const float4 v = __ldg(qb + j2 * qcols);  // T00, dx, dy, dxy
+  const float t = __fadd_rd(u, kMagic);
+  const float b = u - (t - kMagic);
+  const int rb = min(max(__float_as_int(t), kMagicBits), kMagicBits + nt + 2);
+  const float4 v = __ldg(reinterpret_cast<const float4*>(
+      col + (unsigned long long)(unsigned)rb * qrow_bytes));  // T00, dx, dy, dxy
   return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
+}
+
+// EXACT column: weight a and 16 * (clamped column bit pattern) added to the biased view base
+__device__ __forceinline__ unsigned long long quad_col_exact(unsigned long long vbias, float p,
+                                                             int ns, float& a) {
+  const float t = __fadd_rd(p, kMagic);
+  a = p - (t - kMagic);
+  const int cb = min(max(__float_as_int(t), kMagicBits - 2), kMagicBits + ns);
+  return vbias + (unsigned long long)(unsigned)cb * 16ull;
 }
 
 // Column of a sample: clamped origin offset and weight
@@ -142,8 +170,10 @@ __device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a
 // CTA-uniform arguments by every thread of a 256-thread CTA.
 template <int NZ, int INTERP, bool PART>
 __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by, int bz) {
-  __shared__ float s_c1[kQVB], s_s1[kQVB], s_c2[kQVB], s_s2[kQVB];
-  __shared__ int s_jlo[kQVB], s_jhi[kQVB];
+  __shared__ float4 s_cs[kQVB];      // cos, sin of view ia and of its conjugate ia + half
+  __shared__ int2 s_jr[kQVB];        // slices [jlo, jhi) of the chunk whose window holds ia
+  __shared__ float2 s_zb[kQVB];      // EXACT: source z of both views without the fan-angle term
+  __shared__ ulonglong2 s_qv[kQVB];  // EXACT: biased bases of both views (quad_view_bias)
 
   const int tid = threadIdx.y * kQTX + threadIdx.x;
   const int ix = bx * kQTX + threadIdx.x;
@@ -152,9 +182,12 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   const int z0 = (bz % A.zchunks) * NZ;
   const int nzc = min(NZ, A.nz - z0);
 
-  const float xc = ((float)ix - A.wx) * A.dx;
-  const float yc = ((float)iy - A.wy) * A.dy;
-  const float zc0 = ((float)z0 - A.wz) * A.dz;
+  // explicit roundings (_rn, fmaf) wherever a product meets a sum: plain mul/add pairs may be
+  // contracted differently in each instantiation, and the work-list kernel must reproduce a
+  // scan's own launch bit for bit
+  const float xc = __fmul_rn((float)ix - A.wx, A.dx);
+  const float yc = __fmul_rn((float)iy - A.wy, A.dy);
+  const float zc0 = __fmul_rn((float)z0 - A.wz, A.dz);
   const float wt2 = A.wt + 2.0f;
   float zc[NZ];
 #pragma unroll
@@ -187,25 +220,34 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
     __syncthreads();
     if (tid < kQVB && vb + tid < vhi) {
       const int ia = vb + tid;
-      view_trig_pi(betas, ia, s_c1[tid], s_s1[tid]);
-      view_trig_pi(betas, ia + A.half, s_c2[tid], s_s2[tid]);
+      float c1, s1, c2, s2;
+      view_trig_pi(betas, ia, c1, s1);
+      view_trig_pi(betas, ia + A.half, c2, s2);
+      s_cs[tid] = make_float4(c1, s1, c2, s2);
+      if (INTERP == LCT_INTERP_EXACT) {
+        s_zb[tid] = make_float2(fmaf((float)ia, A.dzv, A.z0), fmaf((float)(ia + A.half), A.dzv, A.z0));
+        s_qv[tid] = make_ulonglong2(quad_view_bias(quads + (long long)ia * A.qstride, A.qrow_bytes),
+                                    quad_view_bias(quads + (long long)(ia + A.half) * A.qstride,
+                                                   A.qrow_bytes));
+      }
       int jlo = nzc, jhi = 0;
       for (int j = 0; j < nzc; ++j)
         if (ia >= A.a_min[z0 + j] && ia < A.a_mid[z0 + j]) {
           jlo = min(jlo, j);
           jhi = max(jhi, j + 1);
         }
-      s_jlo[tid] = jlo;
-      s_jhi[tid] = jhi;
+      s_jr[tid] = make_int2(jlo, jhi);
     }
     __syncthreads();
     const int nv = min(kQVB, vhi - vb);
     for (int k = 0; k < nv; ++k) {
       const int ia = vb + k;
-      const int jlo = s_jlo[k], jhi = s_jhi[k];
-      const float cb = s_c1[k], sb = s_s1[k], cb2 = s_c2[k], sb2 = s_s2[k];
+      const int2 jr = s_jr[k];
+      const int jlo = jr.x, jhi = jr.y;
+      const float4 cs = s_cs[k];
+      const float cb = cs.x, sb = cs.y, cb2 = cs.z, sb2 = cs.w;
       // CUDA/Backprojector.cu:53-64, z-invariant part
-      const float phat = -xc * cb - yc * sb;
+      const float phat = fmaf(-xc, cb, -__fmul_rn(yc, sb));
       float theta, delta_p, tho, sq;
       if (INTERP == LCT_INTERP_TEX8) {
         theta = asinf(__fdiv_rn(phat, A.dso));
@@ -213,31 +255,30 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
         tho = __fdiv_rn(theta, A.orbit);
         sq = sqrtf(fmaf(-phat, phat, A.dso2));
       } else {
-        theta = asinf(phat * A.inv_dso);
-        delta_p = theta * A.dso_over_ds;
-        tho = theta * A.inv_orbit;
+        theta = asinf(__fmul_rn(phat, A.inv_dso));
+        delta_p = 0.0f;  // EXACT: the columns are fmaf(+-theta, dso/ds, ws)
+        tho = __fmul_rn(theta, A.inv_orbit);
         const float t = fmaf(-phat, phat, A.dso2);
-        sq = t * rsqrtf(t);
+        sq = __fmul_rn(t, rsqrtf(t));
       }
-      const float zr1 = fmaf((float)ia + tho, A.dzv, A.z0);
-      const float zr2 = fmaf((float)(ia + A.half) - tho, A.dzv, A.z0);
       const float l1 = fmaf(xc, sb, fmaf(-yc, cb, sq));
       const float l2 = fmaf(xc, sb2, fmaf(-yc, cb2, sq));
-      const float k1 = __fdividef(A.kq, l1), k2 = __fdividef(A.kq, l2);
-      const float m1 = -zr1 * k1, m2 = -zr2 * k2;
-      int o1, o2;
-      float a1, a2;
-      quad_col<INTERP>(delta_p + A.ws, A.ns, o1, a1);
-      quad_col<INTERP>(-delta_p + A.ws, A.ns, o2, a2);
-      const float4* q1 = quads + (long long)ia * A.qstride + o1;
-      const float4* q2 = quads + (long long)(ia + A.half) * A.qstride + o2;
       if constexpr (INTERP == LCT_INTERP_EXACT) {
-        // slice j: qhat = h + j kd (one FMA with a constant j, no per-slice z register);
-        // weights halved around one reciprocal -- the factor 2 is restored, exactly, at the
-        // output
-        const float kd1 = k1 * A.dz, kd2 = k2 * A.dz;
-        const float h1 = fmaf(zc0, k1, m1), h2 = fmaf(zc0, k2, m2);
-        const float u1 = h1 + wt2, u2 = h2 + wt2;
+        // source z from the staged per-view term: zr = (ia + tho) dzv + z0
+        const float2 zb = s_zb[k];
+        const ulonglong2 qv = s_qv[k];
+        const float zr1 = fmaf(tho, A.dzv, zb.x), zr2 = fmaf(-tho, A.dzv, zb.y);
+        // slice j: qhat = h + j kd with k = kq / l, kd = k dz (one FMA with a constant j, no
+        // per-slice z register); weights halved around one reciprocal -- the factor 2 is
+        // restored, exactly, at the output
+        const float r1 = __fdividef(1.0f, l1), r2 = __fdividef(1.0f, l2);
+        const float kd1 = __fmul_rn(A.kqdz, r1), kd2 = __fmul_rn(A.kqdz, r2);
+        const float h1 = __fmul_rn(__fsub_rn(zc0, zr1), __fmul_rn(A.kq, r1));
+        const float h2 = __fmul_rn(__fsub_rn(zc0, zr2), __fmul_rn(A.kq, r2));
+        const float u1 = __fadd_rn(h1, wt2), u2 = __fadd_rn(h2, wt2);
+        float a1, a2;
+        const unsigned long long q1 = quad_col_exact(qv.x, fmaf(theta, A.dso_over_ds, A.ws), A.ns, a1);
+        const unsigned long long q2 = quad_col_exact(qv.y, fmaf(-theta, A.dso_over_ds, A.ws), A.ns, a2);
         auto slice_x = [&](int j) {
           const float fj = (float)j;
           const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
@@ -246,8 +287,8 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
           // (1, 0), (1/2, 1/2) -- so w1 s1 + w2 s2 = s2 + w1 (s1 - s2)
           const float in1 = -qh2 * __fdividef(1.0f, qh1 - qh2);
           const float w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
-          const float s1 = quad_sample_exact(q1, A.qcols, A.nt, a1, fmaf(fj, kd1, u1));
-          const float s2 = quad_sample_exact(q2, A.qcols, A.nt, a2, fmaf(fj, kd2, u2));
+          const float s1 = quad_sample_exact(q1, A.qrow_bytes, A.nt, a1, fmaf(fj, kd1, u1));
+          const float s2 = quad_sample_exact(q2, A.qrow_bytes, A.nt, a2, fmaf(fj, kd2, u2));
           acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
         };
         if (jlo == 0 && jhi == NZ) {
@@ -260,6 +301,16 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
         }
         continue;
       }
+      const float zr1 = fmaf((float)ia + tho, A.dzv, A.z0);
+      const float zr2 = fmaf((float)(ia + A.half) - tho, A.dzv, A.z0);
+      const float k1 = __fdividef(A.kq, l1), k2 = __fdividef(A.kq, l2);
+      const float m1 = -zr1 * k1, m2 = -zr2 * k2;
+      int o1, o2;
+      float a1, a2;
+      quad_col<INTERP>(delta_p + A.ws, A.ns, o1, a1);
+      quad_col<INTERP>(-delta_p + A.ws, A.ns, o2, a2);
+      const float4* q1 = quads + (long long)ia * A.qstride + o1;
+      const float4* q2 = quads + (long long)(ia + A.half) * A.qstride + o2;
       auto slice = [&](int j) {
         const float qh1 = fmaf(zc[j], k1, m1), qh2 = fmaf(zc[j], k2, m2);
         const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
@@ -381,6 +432,8 @@ static int build_bp_quad_args(const lct_geom& g, const lct_img& ig, const BpLaun
   a.z0 = g.source_z0;
   a.dzv = g.pitch / (float)g.n_proj_turn;  // CUDA/Backprojector.cu:149
   a.kq = g.dso * (float)g.z_dir / g.dt;
+  a.kqdz = a.kq * ig.dz;
+  a.qrow_bytes = (unsigned)(quad_cols(g.ns) * 16);
   a.wx = ig.wx;
   a.wy = ig.wy;
   a.wz = ig.wz;
