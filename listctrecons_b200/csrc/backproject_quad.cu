@@ -15,6 +15,7 @@
 // for the sample column (phat/dso, theta*dso/ds) and the texture unit's 8-bit weight rules.
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 #include "lct_internal.h"
 #include "tex_emul.cuh"
@@ -47,6 +48,7 @@ struct BpQuadArgs {
   int view_lo, view_hi, part;  // BpLaunch::view_lo / view_hi / part
   float kqdz;           // kq * dz (EXACT: row step per slice = kqdz / l)
   unsigned qrow_bytes;  // bytes per quad row, 16 * qcols
+  int rows_inside_ok;   // 2 wt + 2.5 < nt + 3: |qhat| <= wt puts floor(qhat + wt + 2) in [1, nt + 2]
   int slab_view[kBpMaxSlabs];
   int slab_z0[kBpMaxSlabs];
   int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
@@ -131,12 +133,15 @@ __device__ __forceinline__ unsigned long long quad_view_bias(const float4* view,
 }
 
 // EXACT sample: u = row coordinate + 2 (texel centres at integers), so floor(u) is the quad row;
-// col = quad_view_bias(view) + 16 * (column bit pattern)
+// col = quad_view_bias(view) + 16 * (column bit pattern).  CLAMP false: the caller has shown
+// that 1 <= u < nt + 3 (rows inside the detector), so the row needs no clamp.
+template <bool CLAMP>
 __device__ __forceinline__ float quad_sample_exact(unsigned long long col, unsigned qrow_bytes,
                                                    int nt, float a, float u) {
   const float t = __fadd_rd(u, kMagic);
   const float b = u - (t - kMagic);
-  const int rb = min(max(__float_as_int(t), kMagicBits), kMagicBits + nt + 2);
+  int rb = __float_as_int(t);
+  if (CLAMP) rb = min(max(rb, kMagicBits), kMagicBits + nt + 2);
   const float4 v = __ldg(reinterpret_cast<const float4*>(
       col + (unsigned long long)(unsigned)rb * qrow_bytes));  // T00, dx, dy, dxy
   return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
@@ -149,6 +154,50 @@ __device__ __forceinline__ unsigned long long quad_col_exact(unsigned long long 
   a = p - (t - kMagic);
   const int cb = min(max(__float_as_int(t), kMagicBits - 2), kMagicBits + ns);
   return vbias + (unsigned long long)(unsigned)cb * 16ull;
+}
+
+// Prefetch boxes of one tile in view ia (b1) and its conjugate (b2): {row_lo, row_hi, col_lo,
+// col_hi} in quad rows/columns, from the tile's four corners at its first and last slice, widened
+// by one row and column (the interior can bulge slightly past the corners) and clamped to the
+// view's quads.  Only the L1 prefetch reads them.
+__device__ __forceinline__ void prefetch_boxes(const BpQuadArgs& A, float c1, float s1, float c2,
+                                               float s2, int ia, float x0, float x1, float y0,
+                                               float y1, float zc0, float zcl, int4& b1, int4& b2) {
+  b1 = make_int4(INT_MAX, INT_MIN, INT_MAX, INT_MIN);
+  b2 = b1;
+  const float zb1 = fmaf((float)ia, A.dzv, A.z0), zb2 = fmaf((float)(ia + A.half), A.dzv, A.z0);
+  const float wt2 = A.wt + 2.0f;
+#pragma unroll 1
+  for (int c = 0; c < 4; ++c) {
+    const float x = (c & 1) ? x1 : x0, y = (c >> 1) ? y1 : y0;
+    const float phat = fmaf(-x, c1, -__fmul_rn(y, s1));
+    const float theta = asinf(__fmul_rn(phat, A.inv_dso));
+    const float tho = __fmul_rn(theta, A.inv_orbit);
+    const float t = fmaf(-phat, phat, A.dso2);
+    const float sq = __fmul_rn(t, rsqrtf(t));
+    const float k1 = __fdividef(A.kq, fmaf(x, s1, fmaf(-y, c1, sq)));
+    const float k2 = __fdividef(A.kq, fmaf(x, s2, fmaf(-y, c2, sq)));
+    const float zr1 = fmaf(tho, A.dzv, zb1), zr2 = fmaf(-tho, A.dzv, zb2);
+    for (int e = 0; e < 2; ++e) {
+      const float zc = e ? zcl : zc0;
+      const int r1 = __float2int_rd(fmaf(zc - zr1, k1, wt2));
+      const int r2 = __float2int_rd(fmaf(zc - zr2, k2, wt2));
+      b1.x = min(b1.x, r1); b1.y = max(b1.y, r1);
+      b2.x = min(b2.x, r2); b2.y = max(b2.y, r2);
+    }
+    const int q1 = __float2int_rd(fmaf(theta, A.dso_over_ds, A.ws)) + 2;
+    const int q2 = __float2int_rd(fmaf(-theta, A.dso_over_ds, A.ws)) + 2;
+    b1.z = min(b1.z, q1); b1.w = max(b1.w, q1);
+    b2.z = min(b2.z, q2); b2.w = max(b2.w, q2);
+  }
+  auto fit = [&](int4& b) {
+    b.x = min(max(b.x - 1, 0), A.nt + 2);
+    b.y = min(max(b.y + 1, b.x), A.nt + 2);
+    b.z = min(max(b.z - 1, 0), A.ns + 2);
+    b.w = min(max(b.w + 1, b.z), A.ns + 2);
+  };
+  fit(b1);
+  fit(b2);
 }
 
 // Column of a sample: clamped origin offset and weight
@@ -174,6 +223,8 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   __shared__ int2 s_jr[kQVB];        // slices [jlo, jhi) of the chunk whose window holds ia
   __shared__ float2 s_zb[kQVB];      // EXACT: source z of both views without the fan-angle term
   __shared__ ulonglong2 s_qv[kQVB];  // EXACT: biased bases of both views (quad_view_bias)
+  __shared__ ulonglong2 s_pfb[kQVB]; // EXACT: prefetch box origins of both views
+  __shared__ int4 s_pfs[kQVB];       // EXACT: prefetch box rows and column spans
 
   const int tid = threadIdx.y * kQTX + threadIdx.x;
   const int ix = bx * kQTX + threadIdx.x;
@@ -189,6 +240,12 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   const float yc = __fmul_rn((float)iy - A.wy, A.dy);
   const float zc0 = __fmul_rn((float)z0 - A.wz, A.dz);
   const float wt2 = A.wt + 2.0f;
+  // EXACT prefetch: the tile's corner coordinates and last slice
+  const float xr0 = __fmul_rn((float)(bx * kQTX) - A.wx, A.dx);
+  const float xr1 = __fmul_rn((float)(min(bx * kQTX + kQTX, A.nx) - 1) - A.wx, A.dx);
+  const float yr0 = __fmul_rn((float)(by * kQTY) - A.wy, A.dy);
+  const float yr1 = __fmul_rn((float)(min(by * kQTY + kQTY, A.ny) - 1) - A.wy, A.dy);
+  const float zcl = __fmul_rn((float)(z0 + nzc - 1) - A.wz, A.dz);
   float zc[NZ];
 #pragma unroll
   for (int j = 0; j < NZ; ++j) zc[j] = ((float)(z0 + j) - A.wz) * A.dz;
@@ -226,9 +283,15 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       s_cs[tid] = make_float4(c1, s1, c2, s2);
       if (INTERP == LCT_INTERP_EXACT) {
         s_zb[tid] = make_float2(fmaf((float)ia, A.dzv, A.z0), fmaf((float)(ia + A.half), A.dzv, A.z0));
-        s_qv[tid] = make_ulonglong2(quad_view_bias(quads + (long long)ia * A.qstride, A.qrow_bytes),
-                                    quad_view_bias(quads + (long long)(ia + A.half) * A.qstride,
-                                                   A.qrow_bytes));
+        const float4* v1 = quads + (long long)ia * A.qstride;
+        const float4* v2 = quads + (long long)(ia + A.half) * A.qstride;
+        s_qv[tid] = make_ulonglong2(quad_view_bias(v1, A.qrow_bytes), quad_view_bias(v2, A.qrow_bytes));
+        int4 b1, b2;
+        prefetch_boxes(A, c1, s1, c2, s2, ia, xr0, xr1, yr0, yr1, zc0, zcl, b1, b2);
+        s_pfb[tid] = make_ulonglong2(
+            reinterpret_cast<unsigned long long>(v1) + (unsigned long long)b1.x * A.qrow_bytes + 16ull * b1.z,
+            reinterpret_cast<unsigned long long>(v2) + (unsigned long long)b2.x * A.qrow_bytes + 16ull * b2.z);
+        s_pfs[tid] = make_int4(b1.y - b1.x + 1, b1.w - b1.z, b2.y - b2.x + 1, b2.w - b2.z);
       }
       int jlo = nzc, jhi = 0;
       for (int j = 0; j < nzc; ++j)
@@ -242,6 +305,20 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
     const int nv = min(kQVB, vhi - vb);
     for (int k = 0; k < nv; ++k) {
       const int ia = vb + k;
+      if (INTERP == LCT_INTERP_EXACT && k + 1 < nv) {
+        // the next view's footprint into L1 while this one is sampled (a hint: no result depends
+        // on it, and every address lies inside that view's quads)
+        const int pf_conj = tid >> 7, pf_row = (tid >> 3) & 15, pf_line = tid & 7;
+        const int4 sz = s_pfs[k + 1];
+        const int rows = pf_conj ? sz.z : sz.x, cspan = pf_conj ? sz.w : sz.y;
+        if (pf_row < rows && 8 * pf_line <= cspan + 7) {
+          const ulonglong2 bs = s_pfb[k + 1];
+          const unsigned long long a = (pf_conj ? bs.y : bs.x) +
+                                       (unsigned long long)pf_row * A.qrow_bytes +
+                                       16ull * (unsigned)min(8 * pf_line, cspan);
+          asm volatile("prefetch.global.L1 [%0];" ::"l"(a));
+        }
+      }
       const int2 jr = s_jr[k];
       const int jlo = jr.x, jhi = jr.y;
       const float4 cs = s_cs[k];
@@ -279,25 +356,42 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
         float a1, a2;
         const unsigned long long q1 = quad_col_exact(qv.x, fmaf(theta, A.dso_over_ds, A.ws), A.ns, a1);
         const unsigned long long q2 = quad_col_exact(qv.y, fmaf(-theta, A.dso_over_ds, A.ws), A.ns, a2);
-        auto slice_x = [&](int j) {
+        // INSIDE: both samples of every slice lie within the detector rows (no tests, no selects)
+        auto slice_x = [&](int j, auto inside) {
           const float fj = (float)j;
           const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
-          const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
           // the pair weights sum to one in every case -- (-qh2, qh1) / (qh1 - qh2), (0, 1),
           // (1, 0), (1/2, 1/2) -- so w1 s1 + w2 s2 = s2 + w1 (s1 - s2)
           const float in1 = -qh2 * __fdividef(1.0f, qh1 - qh2);
-          const float w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
-          const float s1 = quad_sample_exact(q1, A.qrow_bytes, A.nt, a1, fmaf(fj, kd1, u1));
-          const float s2 = quad_sample_exact(q2, A.qrow_bytes, A.nt, a2, fmaf(fj, kd2, u2));
+          float w1 = in1;
+          if constexpr (!decltype(inside)::value) {
+            const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
+            w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
+          }
+          constexpr bool kClamp = !decltype(inside)::value;
+          const float s1 = quad_sample_exact<kClamp>(q1, A.qrow_bytes, A.nt, a1, fmaf(fj, kd1, u1));
+          const float s2 = quad_sample_exact<kClamp>(q2, A.qrow_bytes, A.nt, a2, fmaf(fj, kd2, u2));
           acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
         };
+        // qhat(j) = fmaf(j, kd, h) is monotone in j (monotone rounding of a linear function),
+        // so the chunk's first and last slices bound every |qhat|: when both are inside for both
+        // views in every lane of the warp, every out test of the chunk is false and the selects
+        // are skipped with no change to any result.  The row coordinate u = qhat + wt + 2 (equal
+        // to within a few ulps, far below half a row) then lies in (1.5, 2 wt + 2.5), inside the
+        // quad rows when rows_inside_ok.  Plain comparisons: a NaN fails them.
+        bool inside = false;
         if (jlo == 0 && jhi == NZ) {
+          const float e1 = fmaf((float)(NZ - 1), kd1, h1), e2 = fmaf((float)(NZ - 1), kd2, h2);
+          inside = A.rows_inside_ok && fabsf(h1) <= wt && fabsf(e1) <= wt &&
+                   fabsf(h2) <= wt && fabsf(e2) <= wt;
+        }
+        if (__all_sync(0xffffffffu, inside)) {
 #pragma unroll
-          for (int j = 0; j < NZ; ++j) slice_x(j);
+          for (int j = 0; j < NZ; ++j) slice_x(j, std::true_type{});
         } else {
 #pragma unroll
           for (int j = 0; j < NZ; ++j)
-            if (j >= jlo && j < jhi) slice_x(j);
+            if (j >= jlo && j < jhi) slice_x(j, std::false_type{});
         }
         continue;
       }
@@ -434,6 +528,7 @@ static int build_bp_quad_args(const lct_geom& g, const lct_img& ig, const BpLaun
   a.kq = g.dso * (float)g.z_dir / g.dt;
   a.kqdz = a.kq * ig.dz;
   a.qrow_bytes = (unsigned)(quad_cols(g.ns) * 16);
+  a.rows_inside_ok = (2.0 * (double)g.wt + 2.5 < (double)g.nt + 3.0) ? 1 : 0;
   a.wx = ig.wx;
   a.wy = ig.wy;
   a.wz = ig.wz;
