@@ -751,7 +751,8 @@ def run_ours(args, rank, world, dist):
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes": alg_bytes, "launch_ms": bp,
                      "note": "each filtered view is reused ~150x from L1/L2, so HBM is not this "
-                             "kernel's bound: it is issue-bound (79% of issue slots, ncu) -- see "
+                             "kernel's bound: it uses 76% of the issue slots (ncu), the rest "
+                             "mostly waiting on the latency of its 16-byte quad loads -- see "
                              "roofline_onchip and profiles/bp_quad_kernel_*.md"},
         "roofline_onchip": {"bound": "l1", "achieved": l1_achieved, "peak": l1_peak, "unit": "GB/s",
                             "frac": l1_achieved / l1_peak,
