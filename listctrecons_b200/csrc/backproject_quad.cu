@@ -22,7 +22,7 @@
 
 namespace lct {
 
-constexpr int kQTX = 32, kQTY = 8, kQVB = 64;  // views staged per batch
+constexpr int kQTX = 32, kQTY = 8, kQVB = 128;  // views staged per batch
 
 // cos/sin of a view angle in FP64 rounded to float (sincospi: no large-argument reduction)
 __device__ __forceinline__ void view_trig_pi(const float* __restrict__ betas, int v, float& c,
