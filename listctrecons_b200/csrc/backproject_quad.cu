@@ -13,6 +13,11 @@
 //   * views whose window covers every slice of the thread's chunk run an unpredicated loop.
 // EXACT keeps FP64 view trigonometry and full FP32 weights; TEX8 keeps the reference's order
 // for the sample column (phat/dso, theta*dso/ds) and the texture unit's 8-bit weight rules.
+// EXACT also: floor, fraction and index of a sample from one round-down add (no conversions)
+// and one wide multiply-add for its address; per-view terms staged in shared memory 128 views
+// at a time; a warp-uniform path without out tests, selects or row clamps when a chunk's first
+// and last slices project inside the detector rows; an L1 prefetch of the next view's tile
+// footprint; a polynomial asin on tiles within dso / 2 of the axis.
 #include <climits>
 #include <cmath>
 #include <type_traits>
