@@ -722,6 +722,26 @@ def run_ours(args, rank, world, dist):
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         traffic = json.loads(tf.read_text()).get(f"{args.workload}:{args.mode}:{args.interp}")
+    # the other stages against their own rooflines (algorithmic counts; in-library stage times)
+    stage_mean = {k: statistics.mean(t[k] for t in stage) for k in stage[0]}
+    rb_bytes = 4 * g.ns * g.nt * (fc + st.rebinned_views)
+    rb_gbs = rb_bytes / (stage_mean["rebin"] / 1e3) / 1e9
+    f_flop = 2.0 * g.ns * g.ns * st.rebinned_views * g.nt
+    f_tfs = f_flop / (stage_mean["filter"] / 1e3) / 1e12
+    splits = {"bf16x6": 6, "bf16x3": 3}.get(args.filter)
+    tpeak, tkind = measured_peak_tflops()
+    stage_rooflines = {
+        "rebin": {"bound": "hbm", "algorithmic_bytes": rb_bytes, "ms": stage_mean["rebin"],
+                  "achieved": rb_gbs, "peak": peak, "unit": "GB/s", "frac": rb_gbs / peak,
+                  "note": "4 B per fan view read once and per parallel view written once"},
+        "filter": {"bound": "tensor", "algorithmic_flop": f_flop, "ms": stage_mean["filter"],
+                   "achieved": f_tfs, "unit": "TFLOP/s",
+                   "peak": tpeak / splits if splits else None,
+                   "frac": f_tfs / (tpeak / splits) if splits else None,
+                   "note": f"2 ns^2 FLOP per detector row against the {tkind} bf16 dense peak / "
+                           f"{splits or '-'} (the split products issued); the stage time also "
+                           "holds the bf16 plane split and the quad pack"},
+    }
     sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     l1_peak = 128.0 * props.multi_processor_count * sm_mhz * 1e6 / 1e9  # GB/s, 128 B/clk/SM
     l1_achieved = st.voxel_updates * 32 / (bp / 1e3) / 1e9
@@ -741,7 +761,7 @@ def run_ours(args, rank, world, dist):
                        fc * g.nt * g.ns * 4 / 1e9, st.rebinned_views * g.nt * g.ns * 4 / 1e9),
                    "parallelism": f"slab shards x{world}"},
         "s_per_volume": ms / 1e3,
-        "stages_ms": {k: statistics.mean(t[k] for t in stage) for k in stage[0]},
+        "stages_ms": stage_mean,
         "e2e": {"value": e2e, "unit": UNIT, "s_per_volume": e2e_ms / 1e3,
                 "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
         "gpu_launches": launches,
@@ -758,6 +778,7 @@ def run_ours(args, rank, world, dist):
                             "frac": l1_achieved / l1_peak,
                             "note": "32 B per voxel-view update (8 FP32 taps) vs 128 B/clk/SM nominal "
                                     "at the median SM clock"},
+        "stage_rooflines": stage_rooflines,
         "clocks": clk,
     }
     if not args.no_accuracy:
