@@ -99,11 +99,18 @@ __global__ void rebin_fan2par_index_kernel(int* __restrict__ idx, float* __restr
 
 // Scan mode: global parallel view g reads fan coordinate g + s(is), s = alpha(is)/orbit in
 // FP64 (the same shift for every view, so every view of the scan is rebinned identically).
+// A thread makes kRebinViews consecutive views of its column: view g + k reads fan views
+// v0 + k and v0 + k + 1, so kRebinViews outputs take kRebinViews + 1 loads (each view index
+// clamped or zero-filled on its own, exactly as two independent taps would be).
+constexpr int kRebinViews = 4;
+
 template <int INTERP, int ADDR>
 __global__ void __launch_bounds__(256) rebin_fan2par_scan_kernel(
     const float* __restrict__ fan, long long fan_first, long long fan_count,
-    float* __restrict__ par, long long g0, RebinArgs a) {
-  const long long g = g0 + blockIdx.x;
+    float* __restrict__ par, long long g0, long long nviews, RebinArgs a) {
+  const long long lv = (long long)blockIdx.x * kRebinViews;  // first local view of the block
+  const int nk = (int)min((long long)kRebinViews, nviews - lv);
+  const long long g = g0 + lv;
   const int it0 = blockIdx.y * kRebinRows;
   const int it1 = min(a.nt, it0 + kRebinRows);
   const long long plane = (long long)a.nt * a.ns;
@@ -112,23 +119,28 @@ __global__ void __launch_bounds__(256) rebin_fan2par_scan_kernel(
     double fs = floor(s);
     float w = (float)(s - fs);
     if (INTERP == LCT_INTERP_TEX8) w = q8(w);
-    long long v0 = g + (long long)fs - fan_first, v1 = v0 + 1;
-    bool ok0 = true, ok1 = true;
-    if (ADDR == LCT_ADDR_CLAMP) {
-      v0 = v0 < 0 ? 0 : (v0 >= fan_count ? fan_count - 1 : v0);
-      v1 = v1 < 0 ? 0 : (v1 >= fan_count ? fan_count - 1 : v1);
-    } else {
-      ok0 = v0 >= 0 && v0 < fan_count;
-      ok1 = v1 >= 0 && v1 < fan_count;
+    const long long v0 = g + (long long)fs - fan_first;
+    const float* p[kRebinViews + 1];
+    bool ok[kRebinViews + 1];
+#pragma unroll
+    for (int k = 0; k <= kRebinViews; ++k) {
+      long long v = v0 + k;
+      ok[k] = true;
+      if (ADDR == LCT_ADDR_CLAMP)
+        v = v < 0 ? 0 : (v >= fan_count ? fan_count - 1 : v);
+      else
+        ok[k] = v >= 0 && v < fan_count;
+      p[k] = fan + (ok[k] ? v : 0) * plane + is;
     }
-    const float* p0 = fan + v0 * plane + is;
-    const float* p1 = fan + v1 * plane + is;
-    float* o = par + (long long)blockIdx.x * plane + is;
+    float* o = par + lv * plane + is;
     for (int it = it0; it < it1; ++it) {
-      long long r = (long long)it * a.ns;
-      float t0 = ok0 ? __ldg(p0 + r) : 0.0f;
-      float t1 = ok1 ? __ldg(p1 + r) : 0.0f;
-      o[r] = fmaf(w, t1, (1.0f - w) * t0);
+      const long long r = (long long)it * a.ns;
+      float t[kRebinViews + 1];
+#pragma unroll
+      for (int k = 0; k <= kRebinViews; ++k) t[k] = (ok[k] && k <= nk) ? __ldg(p[k] + r) : 0.0f;
+#pragma unroll
+      for (int k = 0; k < kRebinViews; ++k)
+        if (k < nk) o[k * plane + r] = fmaf(w, t[k + 1], (1.0f - w) * t[k]);
     }
   }
 }
@@ -244,16 +256,16 @@ int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long f
   if (nviews <= 0) return LCT_OK;
   if (nviews > 0x7fffffffLL) return LCT_ERR_ARG;
   RebinArgs a = rebin_args(g);
-  dim3 grid((unsigned)nviews, (g.nt + kRebinRows - 1) / kRebinRows);
+  dim3 grid((unsigned)((nviews + kRebinViews - 1) / kRebinViews), (g.nt + kRebinRows - 1) / kRebinRows);
   bool tex = interp == LCT_INTERP_TEX8, clamp = addr == LCT_ADDR_CLAMP;
   if (tex && clamp)
-    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
   else if (tex)
-    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
   else if (clamp)
-    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
   else
-    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
   return launch_status();
 }
 
