@@ -7,7 +7,7 @@ line integrals with Poisson noise (lct_sim_project) -> FDK through lct_recon (th
 -> FDK volume; the target is the phantom voxelised on the FDK voxel grid (lct_voxelise; voxel
 (ix, iy, k) of block b centred at ((ix - wx) dx, (iy - wy) dy, block_start_b + k dz dir)).
 
-Plain FDK is the judge: `plain = calib * fdk`, with `calib` the least-squares scale of the
+Plain FDK is the starting point: `plain = calib * fdk`, with `calib` the least-squares scale of the
 training volumes onto their phantoms (the reference's FDK normalisation is about twice the
 parallel-beam value).  The network sees in_scale * plain (in_scale = 1 / mu_water), predicts a
 residual r, and the corrected volume is plain + r / in_scale wherever |r / in_scale| <= bound
