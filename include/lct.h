@@ -142,14 +142,20 @@ int lct_filter_rows(int ns, const float* d_h, float* d_rows, int64_t nrows, int 
 int lct_backproject_par(const lct_geom* g, const lct_img* ig, const float* d_betas,
                         const float* d_proj, float* d_img, int interp, int addr,
                         lct_stream stream);
+/* Host-side query, no launch: *out = 1 when lct_backproject_par (and the allocation-free
+   variant below) take the quad path for this block -- nz <= 32 and every slice's view window a
+   full rotation, which the reference planner's blocks always have -- else 0 (the general
+   kernel, which needs no scratch). */
+int lct_backproject_par_quad_path(const lct_geom* g, const lct_img* ig, int* out);
 /* No counterpart in the reference.  lct_backproject_par for callers that cannot let the
    library allocate device memory (a host that budgets all device memory itself, an acquisition
    loop that must not stall or fail on an allocation, a plugin host with its own allocator): the
    quad-layout scratch comes from a fixed 64 MiB array in the library that every GPU loading it
    holds until exit, and nothing is allocated.  Blocks needing more than 64 MiB of scratch
    (n_angle*(nt+3)*(ns+3)*16 bytes) return LCT_ERR_SCRATCH before any launch.  All calls on a
-   device share that array: calls that overlap on the GPU race.  The first call on a device
-   resolves the array's address and should come before any stream capture. */
+   device share that array: calls that overlap on the GPU race.  Each call looks up the array's
+   device address for the current device (a host-side lookup); the first call on a device may
+   also load the library's device code there, so make it before any stream capture. */
 int lct_backproject_par_noalloc(const lct_geom* g, const lct_img* ig, const float* d_betas,
                                 const float* d_proj, float* d_img, int interp, int addr,
                                 lct_stream stream);
@@ -378,14 +384,6 @@ void lct_cnn_destroy(lct_cnn* c);
    lct_recon_last_times) and its rejected-voxel count; either pointer may be NULL. */
 int lct_recon_set_learned(lct_recon* r, lct_cnn* c, float bound);
 int lct_recon_learned_info(const lct_recon* r, float* ms, int64_t* rejected);
-
-/* ---------------------------------------------------------------------------------------
- * Diagnostics
- * ------------------------------------------------------------------------------------- */
-/* Samples a 3-D float texture (cudaFilterModeLinear, unnormalised) through the texture
-   hardware: host vol [nz][ny][nx], host coords[3n] (x,y,z), host out[n].  Synchronous. */
-int lct_diag_tex3d_sample(const float* vol, int nx, int ny, int nz, const float* coords,
-                          int64_t n, int addr, float* out);
 
 #ifdef __cplusplus
 }

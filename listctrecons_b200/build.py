@@ -7,6 +7,10 @@ to listctrecons_b200/_build/, and the shared library to listctrecons_b200/liblct
 runtime is linked statically so the library does not depend on the runtime copy another
 library in the process (for example torch) loaded.  Only the ``lct_*`` C entry points are
 exported.
+
+probe/probe.cu becomes listctrecons_b200/liblctprobe.so: measurement probes (the texture unit's
+sampling rule, the L1 load bandwidth) that tests and the benchmark load; nothing in liblct.so
+uses it.
 """
 from __future__ import annotations
 
@@ -22,6 +26,8 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "liblct.so"
+PROBE_SRC = PKG / "probe" / "probe.cu"
+PROBE_LIB = PKG / "liblctprobe.so"
 NVCC = os.environ.get("LCT_NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,14 +79,33 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), srcs))
     newest = max(o.stat().st_mtime for o in objs)
-    if force or not LIB.exists() or LIB.stat().st_mtime < newest:
+    # relink also when the set of sources changed (a removed file leaves a newer library behind)
+    stamp = BUILD / "liblct.objects"
+    names = "\n".join(o.name for o in objs)
+    same_set = stamp.exists() and stamp.read_text() == names
+    if force or not same_set or not LIB.exists() or LIB.stat().st_mtime < newest:
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs)]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
         os.replace(tmp, LIB)
+        stamp.write_text(names)
+    build_probe(force)
     return LIB
+
+
+def build_probe(force: bool = False) -> Path:
+    if force or not PROBE_LIB.exists() or PROBE_LIB.stat().st_mtime < PROBE_SRC.stat().st_mtime:
+        tmp = PROBE_LIB.with_suffix(".so.tmp")
+        cmd = [NVCC, *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler",
+               "-fPIC,-fvisibility=hidden", "-shared", "-cudart", "static", str(PROBE_SRC),
+               "-o", str(tmp)]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {PROBE_SRC.name}:\n{res.stdout}\n{res.stderr}")
+        os.replace(tmp, PROBE_LIB)
+    return PROBE_LIB
 
 
 def main() -> None:

@@ -139,6 +139,7 @@ SIGNATURES: dict[str, tuple] = {
     "lct_filter_rows": (I32, [I32, P, P, I64, I32, P]),
     "lct_backproject_par": (I32, [GP, IP, P, P, P, I32, I32, P]),
     "lct_backproject_par_noalloc": (I32, [GP, IP, P, P, P, I32, I32, P]),
+    "lct_backproject_par_quad_path": (I32, [GP, IP, C.POINTER(I32)]),
     "lct_backproject_pi_ori": (I32, [GP, IP, P, P, P, I32, I32, P]),
     "lct_plan_create": (I32, [C.POINTER(ScanParams), P, P, C.POINTER(P)]),
     "lct_plan_info_get": (I32, [P, C.POINTER(PlanInfo)]),
@@ -159,7 +160,6 @@ SIGNATURES: dict[str, tuple] = {
     "lct_batch_last_times": (I32, [P, P]),
     "lct_batch_destroy": (None, [P]),
     "lct_sim_project": (I32, [P, I32, I32, I32, F32, F32, F32, F32, F32, P, P, I64, I64, F64, U64, P, P]),
-    "lct_diag_tex3d_sample": (I32, [P, I32, I32, I32, P, I64, I32, P]),
     "lct_voxelise": (I32, [P, I32, I32, I32, I32, F64, F64, F64, F64, F64, F64, I32, P, P]),
     "lct_cnn_param_count": (I32, [P]),
     "lct_cnn_create": (I32, [I32, I32, I32, I32, U64, P]),
@@ -209,6 +209,27 @@ def load() -> C.CDLL:
 
 def lib() -> C.CDLL:
     return load()
+
+
+PROBE_PATH = Path(__file__).resolve().parent / "liblctprobe.so"
+_probe = None
+
+
+def load_probe() -> C.CDLL:
+    """liblctprobe.so: measurement probes (texture-unit samples, L1 load bandwidth) used by the
+    tests and the benchmark; nothing in liblct.so depends on it.  Functions return 0 or a
+    cudaError_t value."""
+    global _probe
+    if _probe is None:
+        if not PROBE_PATH.exists():
+            raise ImportError(f"{PROBE_PATH} is missing: build it with `python -m listctrecons_b200.build`")
+        p = C.CDLL(os.fspath(PROBE_PATH))
+        p.lctp_tex3d_sample.restype = I32
+        p.lctp_tex3d_sample.argtypes = [P, I32, I32, I32, P, I64, I32, P]
+        p.lctp_l1_load_gbs.restype = I32
+        p.lctp_l1_load_gbs.argtypes = [I32, I32, I32, C.POINTER(F64), C.POINTER(F64)]
+        _probe = p
+    return _probe
 
 
 def check(status: int, what: str = "") -> None:

@@ -497,6 +497,15 @@ int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaS
 
 using namespace lct;
 
+LCT_API int lct_backproject_par_quad_path(const lct_geom* g, const lct_img* ig, int* out) {
+  int st = check_geom(g);
+  if (st) return st;
+  if ((st = check_img(ig))) return st;
+  if (!out) return LCT_ERR_ARG;
+  *out = (ig->nz <= kBpMaxZ && bp_windows_full(*g, *ig, ig->nz)) ? 1 : 0;
+  return LCT_OK;
+}
+
 LCT_API int lct_backproject_par(const lct_geom* g, const lct_img* ig, const float* d_betas,
                                 const float* d_proj, float* d_img, int interp, int addr,
                                 lct_stream stream) {

@@ -18,38 +18,28 @@
 //     overwrites every element it reads before reading it, so nothing needs clearing, but two
 //     calls whose kernels overlap on the GPU (different streams, no ordering between them) race
 //     on the array: order them, or use lct_backproject_par;
-//   * the first call on each device looks up the array's device address (cudaGetSymbolAddress,
-//     with that device current) and caches it; make that first call before any stream capture.
+//   * every call looks up the array's device address for the current device
+//     (cudaGetSymbolAddress, a host-side lookup, so the address stays right after a device
+//     reset); the first call on a device may also load this library's device code there, so make
+//     it before any stream capture.
 // Windows that are not a full rotation need no scratch: those blocks run the same general
 // kernel lct_backproject_par uses for them.
-#include <mutex>
-
 #include "lct_internal.h"
 
 namespace lct {
 
 constexpr size_t kNoAllocScratchBytes = 64ull << 20;
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) float4 g_noalloc_quads[kNoAllocScratchBytes / sizeof(float4)];
 
 // Device address of the scratch array for the current device.  In host code the name
-// g_noalloc_quads is only a stand-in for the symbol, never a device address.
+// g_noalloc_quads is only a stand-in for the symbol, never a device address.  Looked up on every
+// call: the lookup is host-side, and a cached address would go stale after a device reset.
 static int noalloc_scratch(float4** out) {
-  static std::mutex mu;
-  static float4* ptrs[kNoAllocMaxDevices] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_quads);
   if (e != cudaSuccess) return cuda_status(e);
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return LCT_ERR_UNSUPPORTED;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!ptrs[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_quads);
-    if (e != cudaSuccess) return cuda_status(e);
-    ptrs[dev] = static_cast<float4*>(p);
-  }
-  *out = ptrs[dev];
+  *out = static_cast<float4*>(p);
   return LCT_OK;
 }
 

@@ -438,6 +438,187 @@ void orc_bp_par(const orc_geom* g, const orc_img* ig, const float* betas, const 
   orc_bp_par_rows(g, ig, betas, proj, img, interp, addr, 0, ig->ny);
 }
 
+/* tex3d_lin at a view-axis coordinate on a texel centre (z = ia + 0.5, so the z weight is 0
+   and only layer k contributes): the same operations in the same order as tex3d_lin, without
+   its loop over the second layer. */
+static inline double tex_layer(const float* v, long nx, long ny, long nz, double x, double y,
+                               long k, int interp, int addr) {
+  long i, j;
+  double a, b;
+  lin_axis(x, interp, &i, &a);
+  lin_axis(y, interp, &j, &b);
+  double w[4];
+  if (interp == ORC_TEXEMU) {
+    w[3] = floor(a * b * 256.0 + 0.5) / 256.0;
+    w[1] = a - w[3];
+    w[2] = b - w[3];
+    w[0] = 1.0 - a - b + w[3];
+  } else {
+    w[0] = (1.0 - a) * (1.0 - b);
+    w[1] = a * (1.0 - b);
+    w[2] = (1.0 - a) * b;
+    w[3] = a * b;
+  }
+  double s = 0.0;
+  for (int c = 0; c < 4; ++c) {
+    double wc = 1.0 * w[c];
+    if (wc == 0.0) continue;
+    s += wc * texel3(v, nx, ny, nz, i + (c & 1), j + (c >> 1), k, addr);
+  }
+  return s;
+}
+
+/* orc_bp_par_rows with the loops interchanged: per voxel row iy, views ia outermost, then the
+   row's voxel columns, then every slice whose window holds ia.  The z-invariant terms are
+   evaluated once per (column, view) instead of once per (voxel, view) and a view's samples stay
+   in cache across the row; each voxel still sums its views in increasing ia with the same
+   expressions, so the result is bit-identical to orc_bp_par_rows (pinned by
+   tests/test_oracle_kat.py) and several times faster, which makes whole-slab FP64 checks of
+   full-size volumes practical.  cos/sin of every view angle come from tables evaluated with the
+   same libm calls.  Rows y0, y0 + ystep, ... below y1 are computed; the others are left as they
+   are in img. */
+void orc_bp_par_cols(const orc_geom* g, const orc_img* ig, const float* betas, const float* proj,
+                     double* img, int interp, int addr, int y0, int y1, int ystep) {
+  const long ns = g->ns, nt = g->nt, na = g->n_angle;
+  const int na1_half = g->n_proj_turn / 2;                       /* Backprojector.cu:148 */
+  const float dzv = g->pitch / (float)g->n_proj_turn;            /* Backprojector.cu:149 */
+  const int nz = ig->nz, nx = ig->nx;
+  int* amin = (int*)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+  int* amax = (int*)malloc(sizeof(int) * (size_t)(nz > 0 ? nz : 1));
+  double* cosd = (double*)malloc(sizeof(double) * (size_t)(na > 0 ? na : 1));
+  double* sind = (double*)malloc(sizeof(double) * (size_t)(na > 0 ? na : 1));
+  int lo = (int)na, hi = 0;
+  for (int iz = 0; iz < nz; ++iz) {
+    orc_bp_window(g, ig, iz, dzv, na1_half, &amin[iz], &amax[iz]);
+    if (amax[iz] > amin[iz]) {
+      lo = amin[iz] < lo ? amin[iz] : lo;
+      hi = amax[iz] > hi ? amax[iz] : hi;
+    }
+  }
+  for (long a = 0; a < na; ++a) {
+    cosd[a] = cos((double)betas[a]);
+    sind[a] = sin((double)betas[a]);
+  }
+#pragma omp parallel
+  {
+    double* sum = (double*)malloc(sizeof(double) * (size_t)(nz > 0 ? nz : 1) * (size_t)nx);
+    const int step = ystep > 0 ? ystep : 1;
+    const int nrow = y1 > y0 ? (y1 - y0 + step - 1) / step : 0;
+#pragma omp for schedule(dynamic, 1)
+    for (int r = 0; r < nrow; ++r) {
+      const int iy = y0 + r * step;
+      for (long q = 0; q < (long)nz * nx; ++q) sum[q] = 0.0;
+      for (int ia = lo; ia < hi; ++ia) {
+        /* conjugate candidates: ia + half [0] and ia - half [1] (ia + half when negative) */
+        const int c2[2] = {ia + na1_half, ia - na1_half < 0 ? ia + na1_half : ia - na1_half};
+        const int b2[2] = {c2[0] < g->n_angle ? c2[0] : g->n_angle - 1,
+                           c2[1] < g->n_angle ? c2[1] : g->n_angle - 1};
+        for (int ix = 0; ix < nx; ++ix) {
+          double* acc = sum + (long)ix * nz;
+          if (interp == ORC_TEXEMU) {
+            float xc = ((float)ix - ig->wx) * ig->dx;
+            float yc = ((float)iy - ig->wy) * ig->dy;
+            float cb = (float)cosd[ia], sb = (float)sind[ia];
+            float phat = -xc * cb - yc * sb;
+            float theta = asinf(phat / g->dso);
+            float delta_p = theta * g->dso / g->ds;
+            float p_idx = delta_p + g->ws;
+            float p_idx2 = -delta_p + g->ws;
+            float z_ray = g->source_z0 + ((float)ia + theta / g->orbit) * dzv;
+            float sq = sqrtf(g->dso * g->dso - phat * phat);
+            float lhat = sq + xc * sb - yc * cb;
+            float z_ray2c[2], lhat2c[2];
+            for (int c = 0; c < 2; ++c) {
+              float cb2 = (float)cosd[b2[c]], sb2 = (float)sind[b2[c]];
+              z_ray2c[c] = g->source_z0 + ((float)c2[c] - theta / g->orbit) * dzv;
+              lhat2c[c] = sq + xc * sb2 - yc * cb2;
+            }
+            for (int iz = 0; iz < nz; ++iz) {
+              if (ia < amin[iz] || ia >= amax[iz]) continue;
+              float zc = ((float)iz - ig->wz) * ig->dz;
+              int ia2 = ia + na1_half < amax[iz] ? ia + na1_half : ia - na1_half;
+              const int c = (ia2 < 0 || ia2 == ia + na1_half) ? 0 : 1;
+              ia2 = ia2 < 0 ? ia + na1_half : ia2;
+              float qhat = (zc - z_ray) * g->dso * (float)g->z_dir / (lhat * g->dt);
+              float qhat2 = (zc - z_ray2c[c]) * g->dso * (float)g->z_dir / (lhat2c[c] * g->dt);
+              float q_idx = qhat + g->wt, q_idx2 = qhat2 + g->wt;
+              float ww, ww2;
+              if (fabsf(qhat) > g->wt) {
+                ww = 0.0f;
+                ww2 = 1.0f;
+              } else if (fabsf(qhat2) > g->wt) {
+                ww = 1.0f;
+                ww2 = 0.0f;
+              } else {
+                ww = -qhat2 / (qhat - qhat2);
+                ww2 = qhat / (qhat - qhat2);
+              }
+              double s1 = tex_layer(proj, ns, nt, na, (double)(p_idx + 0.5f),
+                                    (double)(q_idx + 0.5f), ia, interp, addr);
+              double s2 = tex_layer(proj, ns, nt, na, (double)(p_idx2 + 0.5f),
+                                    (double)(q_idx2 + 0.5f), ia2, interp, addr);
+              acc[iz] += s1 * ww + s2 * ww2;
+            }
+          } else {
+            double xc = ((double)ix - ig->wx) * ig->dx;
+            double yc = ((double)iy - ig->wy) * ig->dy;
+            double dso = g->dso, ds = g->ds, dt = g->dt, wt = g->wt, orbit = g->orbit;
+            double dzvd = (double)g->pitch / (double)g->n_proj_turn;
+            double phat = -xc * cosd[ia] - yc * sind[ia];
+            double theta = asin(phat / dso);
+            double delta_p = theta * dso / ds;
+            double p_idx = delta_p + g->ws, p_idx2 = -delta_p + g->ws;
+            double z_ray = g->source_z0 + (ia + theta / orbit) * dzvd;
+            double sq = sqrt(dso * dso - phat * phat);
+            double lhat = sq + xc * sind[ia] - yc * cosd[ia];
+            double z_ray2c[2], lhat2c[2];
+            for (int c = 0; c < 2; ++c) {
+              z_ray2c[c] = g->source_z0 + (c2[c] - theta / orbit) * dzvd;
+              lhat2c[c] = sq + xc * sind[b2[c]] - yc * cosd[b2[c]];
+            }
+            for (int iz = 0; iz < nz; ++iz) {
+              if (ia < amin[iz] || ia >= amax[iz]) continue;
+              double zc = ((double)iz - ig->wz) * ig->dz;
+              int ia2 = ia + na1_half < amax[iz] ? ia + na1_half : ia - na1_half;
+              const int c = (ia2 < 0 || ia2 == ia + na1_half) ? 0 : 1;
+              ia2 = ia2 < 0 ? ia + na1_half : ia2;
+              double qhat = (zc - z_ray) * dso * g->z_dir / (lhat * dt);
+              double qhat2 = (zc - z_ray2c[c]) * dso * g->z_dir / (lhat2c[c] * dt);
+              double ww, ww2;
+              if (fabs(qhat) > wt) {
+                ww = 0.0;
+                ww2 = 1.0;
+              } else if (fabs(qhat2) > wt) {
+                ww = 1.0;
+                ww2 = 0.0;
+              } else {
+                ww = -qhat2 / (qhat - qhat2);
+                ww2 = qhat / (qhat - qhat2);
+              }
+              double s1 = tex_layer(proj, ns, nt, na, p_idx + 0.5, qhat + wt + 0.5, ia,
+                                    ORC_EXACT, addr);
+              double s2 = tex_layer(proj, ns, nt, na, p_idx2 + 0.5, qhat2 + wt + 0.5, ia2,
+                                    ORC_EXACT, addr);
+              acc[iz] += s1 * ww + s2 * ww2;
+            }
+          }
+        }
+      }
+      for (int iz = 0; iz < nz; ++iz)
+        for (int ix = 0; ix < nx; ++ix)
+          img[((long)iz * ig->ny + iy) * nx + ix] =
+              (amax[iz] > amin[iz])
+                  ? sum[(long)ix * nz + iz] * 2.0 * REF_PI / (double)(float)(amax[iz] - amin[iz])
+                  : 0.0;
+    }
+    free(sum);
+  }
+  free(amin);
+  free(amax);
+  free(cosd);
+  free(sind);
+}
+
 /* CUDA/Backprojector.cu:171-250, PI-window backprojection */
 void orc_bp_pi_ori(const orc_geom* g, const orc_img* ig, const float* betas, const float* proj,
                    double* img, int interp, int addr) {

@@ -74,6 +74,7 @@ def lib() -> C.CDLL:
             "orc_bp_window": (None, [G, Ip, C.c_int, C.c_float, C.c_int, P, P]),
             "orc_bp_par_rows": (None, [G, Ip, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int]),
             "orc_bp_par": (None, [G, Ip, P, P, P, C.c_int, C.c_int]),
+            "orc_bp_par_cols": (None, [G, Ip, P, P, P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
             "orc_bp_pi_ori": (None, [G, Ip, P, P, P, C.c_int, C.c_int]),
             "orc_bp_par_rows_f32": (None, [G, Ip, P, P, P, C.c_int, C.c_int]),
             "orc_rebin_filter_f32": (None, [G, P, P, P, C.c_int, C.c_int]),
@@ -196,6 +197,30 @@ def bp_par(g, ig, betas, proj, interp=TEXEMU, addr=BORDER, rows=None):
     lib().orc_bp_par_rows(C.byref(geom_from(g)), C.byref(img_from(ig)), b.ctypes.data,
                           proj.ctypes.data, img.ctypes.data, interp, addr, y0, y1)
     return img
+
+
+def bp_par_cols(g, ig, betas, proj, interp=TEXEMU, addr=BORDER, rows=None, ystep=1):
+    """bp_par with the loops interchanged (z-invariant terms once per voxel column and view):
+    bit-identical to bp_par and several times faster; used for whole-slab checks.  Rows
+    y0, y0 + ystep, ... below y1 are computed, the others stay 0."""
+    proj = _f32(proj)
+    b = _f32(betas)
+    img = np.zeros((ig.nz, ig.ny, ig.nx), dtype=np.float64)
+    y0, y1 = (0, ig.ny) if rows is None else rows
+    lib().orc_bp_par_cols(C.byref(geom_from(g)), C.byref(img_from(ig)), b.ctypes.data,
+                          proj.ctypes.data, img.ctypes.data, interp, addr, y0, y1, ystep)
+    return img
+
+
+def filter_rows_fp64(h, rows):
+    """filter_rows mode 0 as one FP64 matrix product with the Toeplitz matrix
+    T[k][n] = h[n - k + ns] (CUDA/Filter.cu:42-46): the same sums in another order, within
+    1e-14 relative of filter_rows; used for whole-slab checks."""
+    rows = _f32(rows)
+    ns = rows.shape[-1]
+    k = np.arange(ns)
+    T = np.asarray(h, dtype=np.float32).astype(np.float64)[k[None, :] - k[:, None] + ns]
+    return (rows.reshape(-1, ns).astype(np.float64) @ T).reshape(rows.shape)
 
 
 def bp_pi_ori(g, ig, betas, proj, interp=EXACT, addr=BORDER):

@@ -1,7 +1,7 @@
 """Generates the GPU-derived golden fixtures (run on a B200, outputs committed):
 
   tex_hw.npz         samples of the texture unit's linear filter (cudaFilterModeLinear through
-                     lct_diag_tex3d_sample): a 1-D weight sweep and random 2-D bilinear samples
+                     lctp_tex3d_sample in liblctprobe.so): a 1-D weight sweep and random 2-D bilinear samples
                      (z at a texel centre, the backprojector's case) with their volume;
   ref_gpu_small.npz  the reference program's own CUDA path (oracle/_ref/ref_timed, built from
                      the reference sources) on a small helical scan simulated by the CPU oracle:
@@ -46,15 +46,16 @@ def small_scan():
 def tex_samples():
     from listctrecons_b200 import capi
 
-    lib = capi.load()
+    probe = capi.load_probe()
 
     def hw(vol, coords):
         vol = np.ascontiguousarray(vol, np.float32)
         c = np.ascontiguousarray(coords, np.float32)
         out = np.zeros(len(c), np.float32)
         nz, ny, nx = vol.shape
-        capi.check(lib.lct_diag_tex3d_sample(vol.ctypes.data, nx, ny, nz, c.ctypes.data, len(c),
-                                             capi.ADDR_BORDER, out.ctypes.data))
+        rc = probe.lctp_tex3d_sample(vol.ctypes.data, nx, ny, nz, c.ctypes.data, len(c), 0,
+                                     out.ctypes.data)
+        assert rc == 0, f"cudaError {rc}"
         return out
 
     rng = np.random.default_rng(2024)

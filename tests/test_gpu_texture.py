@@ -14,8 +14,9 @@ def _hw(vol, coords, addr):
     vol = np.ascontiguousarray(vol, dtype=np.float32)
     c = np.ascontiguousarray(coords, dtype=np.float32)
     nz, ny, nx = vol.shape
-    capi.check(capi.load().lct_diag_tex3d_sample(vol.ctypes.data, nx, ny, nz, c.ctypes.data, len(c),
-                                                 addr, out.ctypes.data))
+    rc = capi.load_probe().lctp_tex3d_sample(vol.ctypes.data, nx, ny, nz, c.ctypes.data, len(c),
+                                             int(addr == capi.ADDR_CLAMP), out.ctypes.data)
+    assert rc == 0, f"cudaError {rc}"
     return out
 
 
