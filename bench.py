@@ -336,41 +336,61 @@ def oracle_accuracy(w, plan, fan, f0, img, interp, slabs, ystep=1):
 
 
 def plain_gpu(w, geo, ph, ours_value):
-    """The reference program built from its own sources (oracle/_ref/ref_timed) on the same scan:
-    its per-block flow (pageable copies, per-block rebin/filter/BP with texture references).
-    It has no z-range key, so it reconstructs every block the scan allows; its reconstruct()
-    time is scaled to this workload's block count (blocks are equal work)."""
+    """The reference program built from its own sources (oracle/_ref/ref_timed) on the same scan,
+    and the typed drop-in program (reference host code + the product) with both factory type
+    names: its per-block flow (pageable copies, per-block rebin/filter/BP with texture
+    references) and the whole-scan type.  None of them has a z-range key, so each reconstructs
+    every block the scan allows; reconstruct() times are scaled to this workload's block count
+    (blocks are equal work) and include each program's own file reads."""
     import torch
 
-    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.recon import Plan, Reconstruction
     from listctrecons_b200.scan import simulate_gpu, write_scan_files
 
     ref = ROOT / "oracle" / "_ref" / "ref_timed"
+    typed = ROOT / "listctrecons_b200" / "dropin" / "_build" / "LISTCTRecons_b200"
     if not ref.exists():
         return {"unavailable": "oracle/_ref/ref_timed not built"}
     g2 = type(geo)(**{k: getattr(geo, k) for k in geo.__dataclass_fields__})
     g2.max_blocks = 0
-    nb_all = Plan(g2).info.n_blocks
+    plan = Plan(g2)
+    nb_all = plan.info.n_blocks
+    upd = Reconstruction(plan).stats().voxel_updates * w["blocks"] / nb_all
     fan = simulate_gpu(g2, ph, i0=1e5, seed=7).cpu().numpy()
     torch.cuda.empty_cache()
+    runs = {}
     with tempfile.TemporaryDirectory() as td:
         prm = write_scan_files(g2, fan, Path(td) / "data", Path(td) / "out")
         del fan
-        r = subprocess.run([str(ref), str(prm)], capture_output=True, text=True, timeout=1800)
-    if r.returncode != 0:
-        return {"unavailable": "reference program failed: " + r.stdout[-300:]}
-    rec = json.loads(r.stdout.strip().splitlines()[-1])
-    secs = rec["reconstruct_seconds"] * w["blocks"] / rec["n_blocks"]
-    plan = Plan(g2)
-    from listctrecons_b200.recon import Reconstruction
-
-    upd = Reconstruction(plan).stats().voxel_updates * w["blocks"] / nb_all
-    v = upd / secs / 1e9
-    return {"value": v, "unit": UNIT, "s_per_volume": secs, "blocks_timed": rec["n_blocks"],
-            "speedup_e2e": ours_value / v,
-            "what": "reference program (all Src/*.cpp + CUDA/*.cu built from its sources, legacy "
-                    "texture references via a compat header) reconstruct() time incl. its per-block "
-                    "file reads, scaled from its blocks to this workload's"}
+        cmds = [("reference", [str(ref), str(prm)])]
+        if typed.exists():
+            cmds += [("dropin_stages", [str(typed), str(prm), "Helicalfdkramprebingpu"]),
+                     ("dropin_b200", [str(typed), str(prm), "Helicalfdkramprebinb200"])]
+        for name, cmd in cmds:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+            if r.returncode != 0:
+                runs[name] = {"unavailable": f"{name} failed: " + r.stdout[-300:]}
+                continue
+            rec = json.loads(r.stdout.strip().splitlines()[-1])
+            secs = rec["reconstruct_seconds"] * w["blocks"] / rec["n_blocks"]
+            runs[name] = {"value": upd / secs / 1e9, "unit": UNIT, "s_per_volume": secs,
+                          "blocks_timed": rec["n_blocks"]}
+    out = runs.pop("reference")
+    if "value" in out:
+        out["speedup_e2e"] = ours_value / out["value"]
+        out["what"] = ("reference program (all Src/*.cpp + CUDA/*.cu built from its sources, "
+                       "legacy texture references via a compat header) reconstruct() time incl. "
+                       "its per-block file reads, scaled from its blocks to this workload's")
+        for name, v in runs.items():
+            if "value" in v:
+                v["speedup_vs_reference"] = v["value"] / out["value"]
+    out["dropin"] = runs
+    if runs:
+        out["dropin_what"] = ("LISTCTRecons_b200: the reference's host code with the product's "
+                              "stages; Helicalfdkramprebingpu = the reference's per-block flow "
+                              "(TEX8, FP32 filter), Helicalfdkramprebinb200 = the whole-scan "
+                              "type (exact, BF16x6, bounded memory, 64-bit file reader)")
+    return out
 
 
 def cpu_port_sample(w, geo, plan, fan_block_views, budget_s: float):
@@ -639,6 +659,34 @@ def l1_peak_measured() -> dict:
                                    "threads per SM, 16 KiB resident buffer, CUDA events"}
 
 
+def bounded_leg(args, plan, opts, h_fan, h_img, f0, rec, maxr, barrier, stream):
+    """The same reconstruction end to end through a bounded recon (lct_recon_create_bounded:
+    fan, filtered and quad views in rings, a four-slab volume ring), host fan in and host volume
+    out; its device footprint beside the whole-scan recon's; its volume checked bit for bit
+    against the whole-scan run's."""
+    import torch
+
+    from listctrecons_b200.recon import Reconstruction
+
+    b = Reconstruction(plan, bounded=True, **opts)
+    out = torch.empty_like(h_img).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        b.run(h_fan, out, fan_view0=f0)
+    barrier()
+    torch.cuda.synchronize()
+    ms, _ = timed(lambda: b.run(h_fan, out, fan_view0=f0), args.steps, stream)
+    ms = maxr(ms)
+    launches = b.stats().launches * args.steps
+    rec.run(h_fan, h_img, fan_view0=f0)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(out, h_img))
+    upd = b.stats().voxel_updates
+    return {"value": upd / (ms / 1e3) / 1e9, "unit": UNIT, "s_per_volume": ms / 1e3,
+            "device_bytes": b.device_bytes(), "whole_scan_device_bytes": rec.device_bytes(),
+            "bit_identical_to_whole_scan": same,
+            "note": "host fan -> host volume through lct_recon_create_bounded"}, launches
+
+
 def measured_peak_tflops():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -765,7 +813,9 @@ def run_ours(args, rank, world, dist):
                 filter_kind=w["filter_kind"],
                 filter_mode={"fp32": capi.FILTER_FP32, "bf16x3": capi.FILTER_BF16X3, "bf16x6": capi.FILTER_BF16X6}[args.filter],
                 interp=capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT,
-                addr=capi.ADDR_BORDER, bp_nz=args.bp_nz, bp_minb=args.bp_minb)
+                addr=capi.ADDR_BORDER, bp_nz=args.bp_nz, bp_minb=args.bp_minb,
+                bp_sampler={"auto": capi.BP_SAMPLER_AUTO, "quads": capi.BP_SAMPLER_QUADS,
+                            "texture": capi.BP_SAMPLER_TEXTURE}[args.sampler])
     rec = Reconstruction(plan, **opts)
     tuned = rec.autotune() if args.bp_nz == -1 else None  # the choice cached at create
     st = rec.stats()
@@ -841,6 +891,10 @@ def run_ours(args, rank, world, dist):
         learned["note"] = ("timing of the fused correction on this volume; its accuracy against "
                            "the phantom is measured on the learned configuration (--workload cfg4)")
         launches += n
+    bounded = None
+    if not args.no_bounded and opts["mode"] == capi.MODE_SCAN:
+        bounded, n = bounded_leg(args, plan, opts, h_fan, h_img, f0, rec, maxr, barrier, stream)
+        launches += n
     l1 = l1_peak_measured()
     clk = clocks.stop()
 
@@ -880,7 +934,8 @@ def run_ours(args, rank, world, dist):
     alg_gbs = upd * 32 / (bp / 1e3) / 1e9
     own_gbs = upd * 16 / (bp / 1e3) / 1e9
     hbm_gbs = hbm_bytes / (bp / 1e3) / 1e9
-    kernel = "bp_quad_kernel"
+    texture = args.interp == "tex8" and args.sampler in ("auto", "texture")
+    kernel = "bp_tex_kernel" if texture else "bp_quad_kernel"
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -889,6 +944,7 @@ def run_ours(args, rank, world, dist):
         "data": "synthetic (seeded 30-ellipsoid phantom, analytic helical scan + Poisson I0=1e5, simulated on the GPU)",
         "config": workload_config(w, nb, ig.ny, ig.nx, fc, g.nt, g.ns, world),
         "options": {"mode": args.mode, "interp": args.interp, "filter": args.filter,
+                    "sampler": "texture" if texture else "quads",
                     "bp_nz": tuned[0] if tuned else (args.bp_nz or "auto"),
                     "bp_minb": tuned[1] if tuned else (args.bp_minb or "auto"),
                     "bp_tuning": "autotuned at create" if tuned else "fixed",
@@ -899,6 +955,7 @@ def run_ours(args, rank, world, dist):
                 "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
         "gpu_launches": launches,
         "mixed_learned": learned,
+        "bounded": bounded,
         "roofline": {"kernel": kernel, "bound": "l1", "achieved": alg_gbs,
                      "peak": l1.get("gbs"), "unit": "GB/s",
                      "frac": alg_gbs / l1["gbs"] if l1.get("gbs") else None,
@@ -956,6 +1013,9 @@ def main() -> int:
     ap.add_argument("--bp-nz", type=int, default=0,
                     help="slices per backprojection thread: 4, 8, 16; 0 = default; -1 = autotune")
     ap.add_argument("--bp-minb", type=int, default=0)
+    ap.add_argument("--sampler", default="auto", choices=["auto", "quads", "texture"],
+                    help="backprojection sampler: quads (16-byte 2x2 texel loads) or the texture "
+                         "unit (TEX8 only); auto = texture for tex8, quads for exact")
     ap.add_argument("--blocks", type=int, default=0, help="override the blocks per GPU (profiling)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
     ap.add_argument("--ref-budget", type=float, default=4.0,
@@ -963,6 +1023,7 @@ def main() -> int:
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the fused learned-correction leg")
+    ap.add_argument("--no-bounded", action="store_true", help="skip the bounded-memory leg")
     ap.add_argument("--bound", type=float, default=None,
                     help="acceptance-gate bound in units of mu_water (default 10)")
     ap.add_argument("--eval-pairs", type=int, default=4, help="held-out scans (cfg4)")

@@ -212,6 +212,14 @@ typedef struct lct_plan lct_plan;
    CouchPosFile after ViewOffset), copied. */
 int lct_plan_create(const lct_scan_params* p, const float* tube_angles,
                     const float* table_positions, lct_plan** out);
+/* A plan holding planner results computed elsewhere: a host that already planned with the
+   reference's own code (ReconData::convert_from_file_params and BlockInfo::update,
+   Src/DataStructs.cpp:77-250) passes its CTGeom / ImgGeom / ReconInfo as `info` and every
+   block's BlockInfo, and runs exactly those blocks.  info->first_block and info->n_blocks_run
+   select the blocks run; tube_angles / table_positions hold info->n_readings floats (after
+   ViewOffset).  Copies everything. */
+int lct_plan_adopt(const lct_plan_info* info, const lct_block_info* blocks, int n_blocks,
+                   const float* tube_angles, const float* table_positions, lct_plan** out);
 int lct_plan_info_get(const lct_plan* plan, lct_plan_info* out);
 int lct_plan_block(const lct_plan* plan, int b, lct_block_info* out);
 void lct_plan_destroy(lct_plan* plan);
@@ -233,6 +241,16 @@ void lct_plan_destroy(lct_plan* plan);
 #define LCT_BP_PAR 0
 #define LCT_BP_PI_ORI 1
 
+/* Backprojection samplers (scan and block modes with full view windows):
+   QUADS    views repacked as 2x2 texel blocks, one 16-byte load per bilinear sample (either
+            interpolation);
+   TEXTURE  views in a 3-D texture, one hardware fetch per sample (TEX8 only: the reference's own
+            fetch, CUDA/Backprojector.cu:85-86; falls back to QUADS otherwise);
+   AUTO     TEXTURE for TEX8, QUADS for EXACT. */
+#define LCT_BP_SAMPLER_AUTO 0
+#define LCT_BP_SAMPLER_QUADS 1
+#define LCT_BP_SAMPLER_TEXTURE 2
+
 typedef struct lct_recon_opts {
   int mode;          /* LCT_MODE_* */
   int rebinner;      /* LCT_REBIN_* */
@@ -246,6 +264,7 @@ typedef struct lct_recon_opts {
   int bp_nz;         /* backprojection slices per thread: 4, 8, 16; 0 = default (8, or 4 when a
                         view stays active for few slices); -1 = autotune at create */
   int bp_minb;       /* backprojection CTAs per SM the register budget targets: 1-4 (0 = 4) */
+  int bp_sampler;    /* LCT_BP_SAMPLER_*: how the backprojector samples the filtered views */
 } lct_recon_opts;
 
 void lct_recon_opts_default(lct_recon_opts* o);
@@ -265,6 +284,32 @@ int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon
    the device-resident run. */
 int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                   float* image, int image_on_device, lct_stream stream);
+/* Bounded device memory (no reference counterpart for the bound; the reference bounds memory
+   per 32-slice block by re-reading and re-rebinning each block's window, Src/DataReader.cpp:8-19,
+   Src/Reconstructor.cpp:33-48).  Like lct_recon_create, but the fan views, the filtered views
+   and the backprojector's quad views live in rings sized to the slab windows in flight, and a
+   volume written to host memory or a file passes through a ring of four slabs, so the device
+   footprint does not grow with the scan's length.  Each view is still uploaded, rebinned and
+   filtered once, and the volume is bit-identical to lct_recon_create's.  Scan mode with the
+   fan->parallel rebinner, no pre-weighting, the parallel backprojector and BORDER or CLAMP
+   addressing (else LCT_ERR_UNSUPPORTED); no learned correction and no autotuning (bp_nz = -1
+   means the default).  piece_views: views rebinned, filtered and packed per step (0 = 512).
+   Runs: lct_recon_run (host or device fan, host or device volume) and lct_recon_run_file. */
+int lct_recon_create_bounded(const lct_plan* plan, const lct_recon_opts* opts, int piece_views,
+                             lct_recon** out);
+/* Device memory a recon holds (buffers, rings, tensor-core filter operands), bytes. */
+int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
+/* Whole scan from the reference's raw files: RawDataReader::readData (Src/DataReader.cpp:8-19)
+   and RawImageWriter (Src/ImageWriter.cpp:9-43) for every block of the run, with 64-bit offsets.
+   fan_path: the DataInterpFile, fan view v of the scan at byte (v + DataOffset) * nt * ns * 4; a
+   reader thread reads the run's views into pinned chunks that are uploaded as the pipeline
+   needs them.  image_path (or NULL): the volume [n_blocks_run * 32][ny][nx] float32 is written
+   there slab by slab by a writer thread; image (or NULL): host buffer for the volume.  At least
+   one of the two.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
+   correction.  The first call allocates the recon's pinned staging (three fan chunks, two slabs),
+   kept until lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
+int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,
+                       lct_stream stream);
 /* Backprojection autotuner (no reference counterpart): times the kernel's slices-per-thread x
    CTAs-per-SM variants on this recon's buffers, keeps the fastest in the recon, and caches it per
    geometry class for the process.  Synchronous; returns the choice. */

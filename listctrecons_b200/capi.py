@@ -30,6 +30,7 @@ MODE_BLOCK, MODE_SCAN = 0, 1
 REBIN_FAN2PAR, REBIN_NULL, REBIN_PI_ORI = 0, 1, 2
 PW_NONE, PW_PI_ORI = 0, 1
 BP_PAR, BP_PI_ORI = 0, 1
+BP_SAMPLER_AUTO, BP_SAMPLER_QUADS, BP_SAMPLER_TEXTURE = 0, 1, 2
 
 
 class LctError(RuntimeError):
@@ -109,7 +110,7 @@ class ReconOpts(C.Structure):
         ("mode", C.c_int), ("rebinner", C.c_int), ("preweight", C.c_int),
         ("filter_kind", C.c_int), ("window", C.c_int), ("filter_mode", C.c_int),
         ("backprojector", C.c_int), ("interp", C.c_int), ("addr", C.c_int), ("bp_nz", C.c_int),
-        ("bp_minb", C.c_int),
+        ("bp_minb", C.c_int), ("bp_sampler", C.c_int),
     ]
 
 
@@ -142,11 +143,15 @@ SIGNATURES: dict[str, tuple] = {
     "lct_backproject_par_quad_path": (I32, [GP, IP, C.POINTER(I32)]),
     "lct_backproject_pi_ori": (I32, [GP, IP, P, P, P, I32, I32, P]),
     "lct_plan_create": (I32, [C.POINTER(ScanParams), P, P, C.POINTER(P)]),
+    "lct_plan_adopt": (I32, [C.POINTER(PlanInfo), C.POINTER(BlockInfo), I32, P, P, C.POINTER(P)]),
     "lct_plan_info_get": (I32, [P, C.POINTER(PlanInfo)]),
     "lct_plan_block": (I32, [P, I32, C.POINTER(BlockInfo)]),
     "lct_plan_destroy": (None, [P]),
     "lct_recon_opts_default": (None, [C.POINTER(ReconOpts)]),
     "lct_recon_create": (I32, [P, C.POINTER(ReconOpts), C.POINTER(P)]),
+    "lct_recon_create_bounded": (I32, [P, C.POINTER(ReconOpts), I32, C.POINTER(P)]),
+    "lct_recon_device_bytes": (I32, [P, C.POINTER(I64)]),
+    "lct_recon_run_file": (I32, [P, C.c_char_p, C.c_char_p, P, P]),
     "lct_recon_run": (I32, [P, P, I64, I32, P, I32, P]),
     "lct_recon_last_times": (I32, [P, P]),
     "lct_recon_fan_range": (I32, [P, C.POINTER(I64), C.POINTER(I64)]),

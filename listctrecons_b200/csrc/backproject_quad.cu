@@ -39,7 +39,8 @@ __device__ __forceinline__ void view_trig_pi(const float* __restrict__ betas, in
 }
 
 struct BpQuadArgs {
-  const float4* quads;  // view 0 of slab 0's local view 0 is quads + slab_view[s] * qstride
+  const float4* quads;  // slab s's local view ia is view slab_view[s] + ia of quads (mod qring)
+  long long qring;      // > 0: quads is a ring of qring views; 0: linear
   const float* betas;
   float* img;
   long long qstride;    // float4 per view
@@ -59,14 +60,17 @@ struct BpQuadArgs {
   int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
 };
 
-// quad pack: grid (views, nt + 3), block 256 over the ns + 3 quad columns
+// quad pack: grid (views, nt + 3), block 256 over the ns + 3 quad columns; view v goes to slot
+// (vbase + v) mod ring of a ring of quads (ring > 0), else to view v
 template <int ADDR>
 __global__ void __launch_bounds__(256) quad_pack_kernel(const float* __restrict__ rows, int ns,
-                                                        int nt, float4* __restrict__ quads) {
+                                                        int nt, float4* __restrict__ quads,
+                                                        long long vbase, long long ring) {
   const long long v = blockIdx.x;
   const int j = (int)blockIdx.y - 2;
   const float* view = rows + v * (long long)nt * ns;
-  float4* out = quads + v * quad_view_elems(ns, nt) + (long long)blockIdx.y * quad_cols(ns);
+  const long long slot = ring > 0 ? (vbase + v) % ring : v;
+  float4* out = quads + slot * quad_view_elems(ns, nt) + (long long)blockIdx.y * quad_cols(ns);
   auto texel = [&](int r, int c) -> float {
     if (ADDR == LCT_ADDR_CLAMP) {
       r = min(max(r, 0), nt - 1);
@@ -86,15 +90,23 @@ __global__ void __launch_bounds__(256) quad_pack_kernel(const float* __restrict_
 }
 
 int launch_quad_pack(const float* rows, long long views, int ns, int nt, int addr, float4* quads,
-                     cudaStream_t s) {
+                     cudaStream_t s, long long vbase, long long ring) {
   if (views <= 0) return LCT_OK;
-  if (views > 0x7fffffffLL || nt + 3 > 65535) return LCT_ERR_ARG;
+  if (views > 0x7fffffffLL || nt + 3 > 65535 || vbase < 0 || ring < 0) return LCT_ERR_ARG;
+  if (ring > 0 && views > ring) return LCT_ERR_ARG;  // a piece would overwrite itself
   dim3 grid((unsigned)views, nt + 3);
   if (addr == LCT_ADDR_CLAMP)
-    quad_pack_kernel<LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(rows, ns, nt, quads);
+    quad_pack_kernel<LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(rows, ns, nt, quads, vbase, ring);
   else
-    quad_pack_kernel<LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(rows, ns, nt, quads);
+    quad_pack_kernel<LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(rows, ns, nt, quads, vbase, ring);
   return launch_status();
+}
+
+// Base of local view ia of a slab whose local view 0 is view sv of the quads (ring-aware).
+__device__ __forceinline__ const float4* quad_view_ptr(const BpQuadArgs& A, int sv, int ia) {
+  long long v = (long long)sv + ia;
+  if (A.qring > 0) v %= A.qring;
+  return A.quads + v * A.qstride;
 }
 
 // Bilinear sample at origin column already applied to qb (qb = view base + clamped column);
@@ -238,7 +250,7 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
   __shared__ float4 s_cs[kQVB];      // cos, sin of view ia and of its conjugate ia + half
   __shared__ int2 s_jr[kQVB];        // slices [jlo, jhi) of the chunk whose window holds ia
   __shared__ float2 s_zb[kQVB];      // EXACT: source z of both views without the fan-angle term
-  __shared__ ulonglong2 s_qv[kQVB];  // EXACT: biased bases of both views (quad_view_bias)
+  __shared__ ulonglong2 s_qv[kQVB];  // bases of both views (EXACT: biased, quad_view_bias)
   __shared__ ulonglong2 s_pfb[kQVB]; // EXACT: prefetch box origins of both views
   __shared__ int4 s_pfs[kQVB];       // EXACT: prefetch box rows and column spans
 
@@ -279,8 +291,8 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
     vlo = max(vlo, A.view_lo);
     vhi = min(vhi, A.view_hi);
   }
-  const float4* quads = A.quads + (long long)A.slab_view[slab] * A.qstride;
-  const float* betas = A.betas + A.slab_view[slab];
+  const int sv = A.slab_view[slab];
+  const float* betas = A.betas + sv;
   const float wt = A.wt;
 
   float acc[NZ];
@@ -301,10 +313,13 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       view_trig_pi(betas, ia, c1, s1);
       view_trig_pi(betas, ia + A.half, c2, s2);
       s_cs[tid] = make_float4(c1, s1, c2, s2);
+      const float4* v1 = quad_view_ptr(A, sv, ia);
+      const float4* v2 = quad_view_ptr(A, sv, ia + A.half);
+      if (INTERP != LCT_INTERP_EXACT)
+        s_qv[tid] = make_ulonglong2(reinterpret_cast<unsigned long long>(v1),
+                                    reinterpret_cast<unsigned long long>(v2));
       if (INTERP == LCT_INTERP_EXACT) {
         s_zb[tid] = make_float2(fmaf((float)ia, A.dzv, A.z0), fmaf((float)(ia + A.half), A.dzv, A.z0));
-        const float4* v1 = quads + (long long)ia * A.qstride;
-        const float4* v2 = quads + (long long)(ia + A.half) * A.qstride;
         s_qv[tid] = make_ulonglong2(quad_view_bias(v1, A.qrow_bytes), quad_view_bias(v2, A.qrow_bytes));
         int4 b1, b2;
         prefetch_boxes(A, c1, s1, c2, s2, ia, xr0, xr1, yr0, yr1, zc0, zcl, b1, b2);
@@ -427,8 +442,9 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       float a1, a2;
       quad_col<INTERP>(delta_p + A.ws, A.ns, o1, a1);
       quad_col<INTERP>(-delta_p + A.ws, A.ns, o2, a2);
-      const float4* q1 = quads + (long long)ia * A.qstride + o1;
-      const float4* q2 = quads + (long long)(ia + A.half) * A.qstride + o2;
+      const ulonglong2 qb = s_qv[k];
+      const float4* q1 = reinterpret_cast<const float4*>(qb.x) + o1;
+      const float4* q2 = reinterpret_cast<const float4*>(qb.y) + o2;
       auto slice = [&](int j) {
         const float qh1 = fmaf(zc[j], k1, m1), qh2 = fmaf(zc[j], k2, m2);
         const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
@@ -475,6 +491,144 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
 template <int NZ, int INTERP, int MINB, bool PART>
 __global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_constant__ BpQuadArgs A) {
   bp_quad_tile<NZ, INTERP, PART>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// TEX8 sampled by the texture unit itself: the filtered views in a 3-D cudaArray (x = column,
+// y = row, z = view slot; cudaFilterModeLinear, unnormalised, the recon's addressing) and every
+// sample one tex3D at (p_idx + 0.5, q_idx + 0.5, slot + 0.5) -- the reference's own fetch
+// (CUDA/Backprojector.cu:85-86), with z on a texel centre.  The per-view and per-slice arithmetic
+// is the quad kernel's TEX8 path (the reference's order); only the sample differs: the unit's
+// 8-bit weights replace their register emulation.  Slab s's local view ia sits at slot
+// (slab_view[s] + ia) mod qring (qring 0: no wrap).
+template <int NZ, bool PART>
+__device__ __forceinline__ void bp_tex_tile(const BpQuadArgs& A, cudaTextureObject_t tex, int bx,
+                                            int by, int bz) {
+  __shared__ float4 s_cs[kQVB];  // cos, sin of view ia and of its conjugate ia + half
+  __shared__ int2 s_jr[kQVB];    // slices [jlo, jhi) of the chunk whose window holds ia
+  __shared__ float2 s_zs[kQVB];  // texture z of both views (slot + 0.5)
+
+  const int tid = threadIdx.y * kQTX + threadIdx.x;
+  const int ix = bx * kQTX + threadIdx.x;
+  const int iy = by * kQTY + threadIdx.y;
+  const int slab = bz / A.zchunks;
+  const int z0 = (bz % A.zchunks) * NZ;
+  const int nzc = min(NZ, A.nz - z0);
+  const float xc = __fmul_rn((float)ix - A.wx, A.dx);
+  const float yc = __fmul_rn((float)iy - A.wy, A.dy);
+  float zc[NZ];
+#pragma unroll
+  for (int j = 0; j < NZ; ++j) zc[j] = ((float)(z0 + j) - A.wz) * A.dz;
+
+  int vlo = INT_MAX, vhi = INT_MIN;
+  for (int j = 0; j < nzc; ++j) {
+    vlo = min(vlo, A.a_min[z0 + j]);
+    vhi = max(vhi, A.a_mid[z0 + j]);
+  }
+  if (PART) {
+    vlo = max(vlo, A.view_lo);
+    vhi = min(vhi, A.view_hi);
+  }
+  const int sv = A.slab_view[slab];
+  const float* betas = A.betas + sv;
+  const float wt = A.wt;
+
+  float acc[NZ];
+#pragma unroll
+  for (int j = 0; j < NZ; ++j) acc[j] = 0.0f;
+  if (PART && A.part >= kBpMiddle && ix < A.nx && iy < A.ny) {  // continue earlier parts' sums
+    const float* in = A.img + ((long long)(A.slab_z0[slab] + z0) * A.ny + iy) * A.nx + ix;
+#pragma unroll
+    for (int j = 0; j < NZ; ++j)
+      if (j < nzc) acc[j] = in[j * (long long)A.nx * A.ny];
+  }
+
+  for (int vb = vlo; vb < vhi; vb += kQVB) {
+    __syncthreads();
+    if (tid < kQVB && vb + tid < vhi) {
+      const int ia = vb + tid;
+      float c1, s1, c2, s2;
+      view_trig_pi(betas, ia, c1, s1);
+      view_trig_pi(betas, ia + A.half, c2, s2);
+      s_cs[tid] = make_float4(c1, s1, c2, s2);
+      long long v1 = (long long)sv + ia, v2 = v1 + A.half;
+      if (A.qring > 0) {
+        v1 %= A.qring;
+        v2 %= A.qring;
+      }
+      s_zs[tid] = make_float2((float)v1 + 0.5f, (float)v2 + 0.5f);
+      int jlo = nzc, jhi = 0;
+      for (int j = 0; j < nzc; ++j)
+        if (ia >= A.a_min[z0 + j] && ia < A.a_mid[z0 + j]) {
+          jlo = min(jlo, j);
+          jhi = max(jhi, j + 1);
+        }
+      s_jr[tid] = make_int2(jlo, jhi);
+    }
+    __syncthreads();
+    const int nv = min(kQVB, vhi - vb);
+    for (int k = 0; k < nv; ++k) {
+      const int ia = vb + k;
+      const int2 jr = s_jr[k];
+      const int jlo = jr.x, jhi = jr.y;
+      const float4 cs = s_cs[k];
+      const float2 zs = s_zs[k];
+      const float cb = cs.x, sb = cs.y, cb2 = cs.z, sb2 = cs.w;
+      // CUDA/Backprojector.cu:53-64, z-invariant part, in the reference's order
+      const float phat = fmaf(-xc, cb, -__fmul_rn(yc, sb));
+      const float theta = asinf(__fdiv_rn(phat, A.dso));
+      const float delta_p = __fdiv_rn(__fmul_rn(theta, A.dso), A.ds);
+      const float tho = __fdiv_rn(theta, A.orbit);
+      const float sq = sqrtf(fmaf(-phat, phat, A.dso2));
+      const float l1 = fmaf(xc, sb, fmaf(-yc, cb, sq));
+      const float l2 = fmaf(xc, sb2, fmaf(-yc, cb2, sq));
+      const float zr1 = fmaf((float)ia + tho, A.dzv, A.z0);
+      const float zr2 = fmaf((float)(ia + A.half) - tho, A.dzv, A.z0);
+      const float k1 = __fdividef(A.kq, l1), k2 = __fdividef(A.kq, l2);
+      const float m1 = -zr1 * k1, m2 = -zr2 * k2;
+      const float x1 = __fadd_rn(delta_p + A.ws, 0.5f), x2 = __fadd_rn(-delta_p + A.ws, 0.5f);
+      auto slice = [&](int j) {
+        const float qh1 = fmaf(zc[j], k1, m1), qh2 = fmaf(zc[j], k2, m2);
+        const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
+        const float r = __fdividef(2.0f, qh1 - qh2);
+        float w1 = -qh2 * r, w2 = qh1 * r;
+        w1 = out1 ? (out2 ? 1.0f : 0.0f) : (out2 ? 2.0f : w1);
+        w2 = out1 ? (out2 ? 1.0f : 2.0f) : (out2 ? 0.0f : w2);
+        const float s1 = tex3D<float>(tex, x1, __fadd_rn(qh1 + wt, 0.5f), zs.x);
+        const float s2 = tex3D<float>(tex, x2, __fadd_rn(qh2 + wt, 0.5f), zs.y);
+        acc[j] = fmaf(w1, s1, fmaf(w2, s2, acc[j]));
+      };
+      if (jlo == 0 && jhi == NZ) {
+#pragma unroll
+        for (int j = 0; j < NZ; ++j) slice(j);
+      } else {
+#pragma unroll
+        for (int j = 0; j < NZ; ++j)
+          if (j >= jlo && j < jhi) slice(j);
+      }
+    }
+  }
+
+  if (ix < A.nx && iy < A.ny) {
+    float* out = A.img + ((long long)(A.slab_z0[slab] + z0) * A.ny + iy) * A.nx + ix;
+    const long long plane = (long long)A.nx * A.ny;
+    const bool raw = PART && (A.part == kBpFirst || A.part == kBpMiddle);  // more parts follow
+#pragma unroll
+    for (int j = 0; j < NZ; ++j) {
+      if (j < nzc && raw) {
+        out[j * plane] = acc[j];
+      } else if (j < nzc) {
+        const int span = A.a_max[z0 + j] - A.a_min[z0 + j];
+        // CUDA/Backprojector.cu:96 in double; x2 restores the pair doubling
+        out[j * plane] = span > 0 ? (float)((double)(acc[j] * 2.0f) * kRefPi / (double)(float)span) : 0.0f;
+      }
+    }
+  }
+}
+
+template <int NZ, int MINB, bool PART>
+__global__ void __launch_bounds__(kQTX* kQTY, MINB)
+    bp_tex_kernel(const __grid_constant__ BpQuadArgs A, cudaTextureObject_t tex) {
+  bp_tex_tile<NZ, PART>(A, tex, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Persistent work list over several scans: item i belongs to the scan s with
@@ -528,6 +682,8 @@ static int build_bp_quad_args(const lct_geom& g, const lct_img& ig, const BpLaun
   if (L.nz <= 0 || L.nz > kBpMaxZ || L.n_slabs <= 0 || L.n_slabs > kBpMaxSlabs) return LCT_ERR_ARG;
   if (!bp_windows_full(g, ig, L.nz)) return LCT_ERR_UNSUPPORTED;
   a.quads = quads;
+  a.qring = L.quad_ring;
+  if (a.qring < 0) return LCT_ERR_ARG;
   a.betas = L.betas;
   a.img = L.img;
   a.qstride = quad_view_elems(g.ns, g.nt);
@@ -619,6 +775,41 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
   }
 #undef LCT_BPQ_NZ
 #undef LCT_BPQ
+  return launch_status();
+}
+
+int launch_bp_par_texture(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                          cudaTextureObject_t tex, cudaStream_t s) {
+  if (L.interp != LCT_INTERP_TEX8) return LCT_ERR_UNSUPPORTED;
+  static thread_local BpQuadArgs a;
+  int nzt = 8;
+  int st = build_bp_quad_args(g, ig, L, nullptr, a, nzt);
+  if (st) return st;
+  dim3 grid(a.gx, a.gy, a.gz);
+  dim3 block(kQTX, kQTY);
+  int minb = L.minb;
+  if (minb < 1 || minb > 4) minb = 4;
+  const bool part = L.part != kBpWhole || L.view_lo > 0 || L.view_hi < (1 << 30);
+#define LCT_BPT(NZV, MB)                                                         \
+  do {                                                                           \
+    if (part) bp_tex_kernel<NZV, MB, true><<<grid, block, 0, s>>>(a, tex);       \
+    else bp_tex_kernel<NZV, MB, false><<<grid, block, 0, s>>>(a, tex);           \
+  } while (0)
+#define LCT_BPT_NZ(NZV)                  \
+  do {                                   \
+    switch (minb) {                      \
+      case 2: LCT_BPT(NZV, 2); break;    \
+      case 3: LCT_BPT(NZV, 3); break;    \
+      default: LCT_BPT(NZV, 4);          \
+    }                                    \
+  } while (0)
+  switch (nzt) {
+    case 4: LCT_BPT_NZ(4); break;
+    case 16: LCT_BPT_NZ(16); break;
+    default: LCT_BPT_NZ(8);
+  }
+#undef LCT_BPT_NZ
+#undef LCT_BPT
   return launch_status();
 }
 

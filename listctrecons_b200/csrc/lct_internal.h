@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "lct.h"
@@ -69,6 +70,9 @@ struct BpLaunch {
   // whole launch
   int view_lo = 0, view_hi = 1 << 30;
   int part = 0;
+  // quad kernel only: > 0 when the quads are a ring of that many views (slab s's local view ia
+  // at slot (slab_view[s] + ia) mod quad_ring; bounded-memory runs); 0: linear
+  long long quad_ring = 0;
 };
 enum BpPart : int { kBpWhole = 0, kBpFirst = 1, kBpMiddle = 2, kBpLast = 3 };
 int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaStream_t s);
@@ -81,11 +85,30 @@ int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaS
 // ring makes every clamped origin valid.
 LCT_HD inline long long quad_cols(int ns) { return (long long)ns + 3; }
 LCT_HD inline long long quad_view_elems(int ns, int nt) { return (long long)(nt + 3) * (ns + 3); }
+// ring > 0: quads is a ring of `ring` views and rows view v is packed into slot
+// (vbase + v) mod ring; 0: into view v.
 int launch_quad_pack(const float* rows, long long views, int ns, int nt, int addr, float4* quads,
-                     cudaStream_t s);
+                     cudaStream_t s, long long vbase = 0, long long ring = 0);
 // Backprojection from quad-layout views (full windows only; L.proj is ignored, L.quads used).
 int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
                         const float4* quads, cudaStream_t s);
+// Backprojection sampled by the texture unit (TEX8 only): tex holds the filtered views as a
+// 3-D array, slab s's local view ia at z slot (slab_view[s] + ia) mod L.quad_ring (0: no wrap).
+int launch_bp_par_texture(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                          cudaTextureObject_t tex, cudaStream_t s);
+// A 3-D float texture of `depth` filtered views (x = column, y = row, z = view slot) with linear
+// filtering and BORDER or CLAMP addressing; filled from linear views by view_texture_fill
+// (slot0 onward, wrapping at depth).
+struct ViewTexture {
+  cudaArray_t arr = nullptr;
+  cudaTextureObject_t tex = 0;
+  int ns = 0, nt = 0;
+  long long depth = 0;
+};
+int view_texture_create(ViewTexture& t, int ns, int nt, long long depth, int addr);
+void view_texture_destroy(ViewTexture& t);
+int view_texture_fill(const ViewTexture& t, const float* rows, long long views, long long slot0,
+                      cudaStream_t s);
 // True when every slice window of the block is a full rotation (the pairs kernels apply).
 bool bp_windows_full(const lct_geom& g, const lct_img& ig, int nz);
 // Work-list backprojection over several scans (batch): per-scan kernel arguments are built on
@@ -100,9 +123,11 @@ int launch_bp_quad_worklist(const void* d_args, const int* d_prefix, int n_scans
 // Rebinning, scan mode: each global parallel view g in [g0, g0 + nviews) is interpolated
 // from the fan buffer whose view 0 is global fan view `fan_first`, with the view shift of
 // column is taken from an FP64 table (alpha(is)/orbit), identical for every view.
+// fan_ring > 0: d_fan is a ring of fan_ring views (fan view v - fan_first at slot v mod ring).
 int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long fan_first,
                               long long fan_count, float* d_par, long long g0,
-                              long long nviews, int interp, int addr, cudaStream_t s);
+                              long long nviews, int interp, int addr, cudaStream_t s,
+                              long long fan_ring = 0);
 
 // BF16x3 tensor-core filter with caller-owned scratch (filter_tc.cu): tc_scratch_bytes() for
 // rows_cap rows; tc_build_toeplitz once per taps, then tc_filter per batch of rows (in place).

@@ -233,6 +233,47 @@ LCT_API int lct_plan_create(const lct_scan_params* p, const float* tube_angles,
   return LCT_OK;
 }
 
+LCT_API int lct_plan_adopt(const lct_plan_info* info, const lct_block_info* blocks, int n_blocks,
+                           const float* tube_angles, const float* table_positions,
+                           lct_plan** out) {
+  if (!info || !blocks || !tube_angles || !table_positions || !out) return LCT_ERR_ARG;
+  *out = nullptr;
+  int st = check_geom(&info->ctg);
+  if (st) return st;
+  if ((st = check_img(&info->ig))) return st;
+  if (info->ig.nz != kBlockSlices || info->n_readings <= 0) return LCT_ERR_ARG;
+  if (n_blocks <= 0 || n_blocks != info->n_blocks) return LCT_ERR_ARG;
+  if (info->first_block < 0 || info->n_blocks_run <= 0 ||
+      info->first_block + info->n_blocks_run > n_blocks)
+    return LCT_ERR_ARG;
+  // (the views a run reads are checked against the data by lct_recon_create, as for any plan)
+  lct_plan* P = new (std::nothrow) lct_plan;
+  if (!P) return LCT_ERR_ALLOC;
+  std::memset(&P->p, 0, sizeof(P->p));
+  P->p.ns = info->ctg.ns;
+  P->p.nt = info->ctg.nt;
+  P->p.ds = info->ctg.ds;
+  P->p.dt = info->ctg.dt;
+  P->p.pitch_value = info->ctg.pitch;
+  P->p.nx = info->ig.nx;
+  P->p.ny = info->ig.ny;
+  P->p.dx = info->ig.dx;
+  P->p.dz = info->ig.dz;
+  P->p.readings = info->n_readings;
+  P->p.data_offset = info->data_offset;
+  P->p.r_src_to_iso = info->ctg.dso;
+  P->p.central_channel = info->ctg.ws;
+  P->p.n_proj_turn = info->ctg.n_proj_turn;
+  P->p.first_block = info->first_block;
+  P->p.max_blocks = info->n_blocks_run;
+  P->angles.assign(tube_angles, tube_angles + info->n_readings);
+  P->zpos.assign(table_positions, table_positions + info->n_readings);
+  P->info = *info;
+  P->blocks.assign(blocks, blocks + n_blocks);
+  *out = P;
+  return LCT_OK;
+}
+
 LCT_API int lct_plan_info_get(const lct_plan* plan, lct_plan_info* out) {
   if (!plan || !out) return LCT_ERR_ARG;
   *out = plan->info;

@@ -102,11 +102,13 @@ __global__ void rebin_fan2par_index_kernel(int* __restrict__ idx, float* __restr
 // A thread makes kRebinViews consecutive views of its column: view g + k reads fan views
 // v0 + k and v0 + k + 1, so kRebinViews outputs take kRebinViews + 1 loads (each view index
 // clamped or zero-filled on its own, exactly as two independent taps would be).
+// fan_ring > 0: the fan buffer is a ring of fan_ring views, fan view v (relative to fan_first)
+// at slot v mod fan_ring (bounded-memory runs); 0: linear.
 constexpr int kRebinViews = 4;
 
 template <int INTERP, int ADDR>
 __global__ void __launch_bounds__(256) rebin_fan2par_scan_kernel(
-    const float* __restrict__ fan, long long fan_first, long long fan_count,
+    const float* __restrict__ fan, long long fan_first, long long fan_count, long long fan_ring,
     float* __restrict__ par, long long g0, long long nviews, RebinArgs a) {
   const long long lv = (long long)blockIdx.x * kRebinViews;  // first local view of the block
   const int nk = (int)min((long long)kRebinViews, nviews - lv);
@@ -130,7 +132,9 @@ __global__ void __launch_bounds__(256) rebin_fan2par_scan_kernel(
         v = v < 0 ? 0 : (v >= fan_count ? fan_count - 1 : v);
       else
         ok[k] = v >= 0 && v < fan_count;
-      p[k] = fan + (ok[k] ? v : 0) * plane + is;
+      if (!ok[k]) v = 0;
+      if (fan_ring > 0) v %= fan_ring;
+      p[k] = fan + v * plane + is;
     }
     float* o = par + lv * plane + is;
     for (int it = it0; it < it1; ++it) {
@@ -252,20 +256,21 @@ __global__ void __launch_bounds__(256) weight_pi_ori_kernel(float* __restrict__ 
 
 int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long fan_first,
                               long long fan_count, float* d_par, long long g0,
-                              long long nviews, int interp, int addr, cudaStream_t s) {
+                              long long nviews, int interp, int addr, cudaStream_t s,
+                              long long fan_ring) {
   if (nviews <= 0) return LCT_OK;
-  if (nviews > 0x7fffffffLL) return LCT_ERR_ARG;
+  if (nviews > 0x7fffffffLL || fan_ring < 0) return LCT_ERR_ARG;
   RebinArgs a = rebin_args(g);
   dim3 grid((unsigned)((nviews + kRebinViews - 1) / kRebinViews), (g.nt + kRebinRows - 1) / kRebinRows);
   bool tex = interp == LCT_INTERP_TEX8, clamp = addr == LCT_ADDR_CLAMP;
   if (tex && clamp)
-    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
   else if (tex)
-    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
   else if (clamp)
-    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
   else
-    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, d_par, g0, nviews, a);
+    rebin_fan2par_scan_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
   return launch_status();
 }
 

@@ -38,6 +38,7 @@ static void free_recon(lct_recon* r) {
   cudaFree(r->d_h);
   cudaFree(r->d_img);
   cudaFree(r->d_quad);
+  view_texture_destroy(r->vtex);
   cudaFree(r->d_tc);
   cudaFree(r->d_plain);
   for (auto& e : r->ev)
@@ -47,23 +48,8 @@ static void free_recon(lct_recon* r) {
   for (auto& e : r->sev)
     if (e) cudaEventDestroy(e);
   streams_destroy(r->ss);
+  recon_free_bounded(r);
   delete r;
-}
-
-static int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
-  if (requested == 4 || requested == 8 || requested == 16) return requested;  // else default
-  // slices a view stays active for: (feed/2) / dz; measured best: 8 unless views are active
-  // for only a few slices
-  const double act = 0.5 * (double)g.pitch / (double)ig.dz;
-  return act < 6.0 ? 4 : 8;
-}
-
-// kernels one filter call launches
-static int filter_launches(int mode) { return mode == LCT_FILTER_FP32 ? 1 : 2; }
-
-static int block_addr(const lct_recon* r, int b) {
-  if (r->o.addr == LCT_ADDR_LEGACY) return b == 0 ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
-  return r->o.addr;
 }
 
 }  // namespace lct
@@ -83,9 +69,13 @@ LCT_API void lct_recon_opts_default(lct_recon_opts* o) {
   o->addr = LCT_ADDR_BORDER;
   o->bp_nz = 0;
   o->bp_minb = 0;
+  o->bp_sampler = LCT_BP_SAMPLER_AUTO;
 }
 
-LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out) {
+namespace lct {
+
+// Options check and the plan-derived fields of a recon (no allocation).
+int recon_setup(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out) {
   if (!plan || !out) return LCT_ERR_ARG;
   *out = nullptr;
   lct_recon_opts o;
@@ -145,42 +135,87 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
     }
     r->voxel_updates = per_block * nb;
   }
+  r->quads = o.backprojector == LCT_BP_PAR && bp_windows_full(g, r->info.ig, kBlockSlices);
+  r->tex_bp = want_texture(o, r->quads);
+  *out = r;
+  return LCT_OK;
+}
 
-  int st = LCT_OK;
+// Allocations every recon has: view angles, taps, the tensor-core filter's operands for
+// tc_rows rows (BF16 modes), timing events.
+int recon_alloc_common(lct_recon* r, const lct_plan* plan) {
+  const lct_geom& g = r->info.ctg;
+  const long long readings = r->info.n_readings;
+  int st;
+  auto track = [&](size_t bytes) { r->device_bytes += (long long)bytes; };
+  if ((st = cuda_status(cudaMalloc(&r->d_betas, sizeof(float) * readings)))) return st;
+  track(sizeof(float) * readings);
+  if ((st = cuda_status(cudaMalloc(&r->d_h, sizeof(float) * 2 * g.ns)))) return st;
+  track(sizeof(float) * 2 * g.ns);
+  if ((st = cuda_status(cudaMemcpy(r->d_betas, plan_angles(plan), sizeof(float) * readings,
+                                   cudaMemcpyHostToDevice))))
+    return st;
+  std::vector<float> h(2 * (size_t)g.ns);
+  if ((st = lct_filter_taps(r->o.filter_kind, r->o.window, g.ns, g.ds, h.data()))) return st;
+  if ((st = cuda_status(cudaMemcpy(r->d_h, h.data(), sizeof(float) * h.size(),
+                                   cudaMemcpyHostToDevice))))
+    return st;
+  if (r->o.filter_mode != LCT_FILTER_FP32) {
+    const size_t b = tc_scratch_bytes(g.ns, r->tc_rows, r->o.filter_mode);
+    if ((st = cuda_status(cudaMalloc(&r->d_tc, b)))) return st;
+    track(b);
+    if ((st = tc_build_toeplitz(g.ns, r->d_h, r->d_tc, r->o.filter_mode, 0))) return st;
+    if ((st = cuda_status(cudaDeviceSynchronize()))) return st;
+  }
+  for (auto& e : r->ev)
+    if ((st = cuda_status(cudaEventCreate(&e)))) return st;
+  return LCT_OK;
+}
+
+int recon_alloc_status(int st) {
+  return st == LCT_ERR_CUDA && lct_last_cuda_error() == cudaErrorMemoryAllocation ? LCT_ERR_ALLOC : st;
+}
+
+}  // namespace lct
+
+LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out) {
+  lct_recon* r = nullptr;
+  int st = recon_setup(plan, opts, &r);
+  if (st) return st;
+  const lct_recon_opts& o = r->o;
+  const lct_geom& g = r->info.ctg;
+  const int nb = r->info.n_blocks_run;
   const long long par_views = o.mode == LCT_MODE_SCAN ? r->g_count : g.n_angle;
   const size_t img_elems = (size_t)nb * kBlockSlices * r->info.ig.nx * r->info.ig.ny;
+  auto alloc = [&](void** p, size_t bytes) {
+    int e = cuda_status(cudaMalloc(p, bytes));
+    if (!e) r->device_bytes += (long long)bytes;
+    return e;
+  };
   do {
-    if ((st = cuda_status(cudaMalloc(&r->d_fan, sizeof(float) * r->fan_count * r->plane)))) break;
-    if ((st = cuda_status(cudaMalloc(&r->d_par, sizeof(float) * par_views * r->plane)))) break;
-    if ((st = cuda_status(cudaMalloc(&r->d_betas, sizeof(float) * readings)))) break;
-    if ((st = cuda_status(cudaMalloc(&r->d_h, sizeof(float) * 2 * g.ns)))) break;
-    if ((st = cuda_status(cudaMalloc(&r->d_img, sizeof(float) * img_elems)))) break;
-    r->quads = o.backprojector == LCT_BP_PAR && bp_windows_full(g, r->info.ig, kBlockSlices);
-    if (r->quads &&
-        (st = cuda_status(cudaMalloc(&r->d_quad, sizeof(float4) * par_views *
-                                                     quad_view_elems(g.ns, g.nt)))))
-      break;
-    if ((st = cuda_status(cudaMemcpy(r->d_betas, plan_angles(plan), sizeof(float) * readings,
-                                     cudaMemcpyHostToDevice))))
-      break;
-    std::vector<float> h(2 * (size_t)g.ns);
-    if ((st = lct_filter_taps(o.filter_kind, o.window, g.ns, g.ds, h.data()))) break;
-    if ((st = cuda_status(cudaMemcpy(r->d_h, h.data(), sizeof(float) * h.size(),
-                                     cudaMemcpyHostToDevice))))
-      break;
-    if (o.filter_mode != LCT_FILTER_FP32) {
-      r->tc_rows = par_views * g.nt;
-      if ((st = cuda_status(cudaMalloc(&r->d_tc, tc_scratch_bytes(g.ns, r->tc_rows, o.filter_mode)))))
-        break;
-      if ((st = tc_build_toeplitz(g.ns, r->d_h, r->d_tc, o.filter_mode, 0))) break;
-      if ((st = cuda_status(cudaDeviceSynchronize()))) break;
+    if ((st = alloc((void**)&r->d_fan, sizeof(float) * r->fan_count * r->plane))) break;
+    if ((st = alloc((void**)&r->d_par, sizeof(float) * par_views * r->plane))) break;
+    if ((st = alloc((void**)&r->d_img, sizeof(float) * img_elems))) break;
+    if (r->tex_bp) {
+      // a 3-D texture holds at most the device's depth limit of views: beyond it, quads
+      if ((st = view_texture_create(r->vtex, g.ns, g.nt, par_views,
+                                    o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER))) {
+        if (st != LCT_ERR_UNSUPPORTED) break;
+        r->tex_bp = false;
+        st = LCT_OK;
+      } else {
+        r->device_bytes += (long long)sizeof(float) * par_views * r->plane;
+      }
     }
-    for (auto& e : r->ev)
-      if ((st = cuda_status(cudaEventCreate(&e)))) break;
+    if (r->quads && !r->tex_bp &&
+        (st = alloc((void**)&r->d_quad, sizeof(float4) * par_views * quad_view_elems(g.ns, g.nt))))
+      break;
+    if (o.filter_mode != LCT_FILTER_FP32) r->tc_rows = par_views * g.nt;
+    st = recon_alloc_common(r, plan);
   } while (0);
   if (st) {
     free_recon(r);
-    return st == LCT_ERR_CUDA && lct_last_cuda_error() == cudaErrorMemoryAllocation ? LCT_ERR_ALLOC : st;
+    return recon_alloc_status(st);
   }
   if (o.bp_nz == -1 && (st = lct_recon_autotune(r, nullptr, nullptr))) {
     free_recon(r);
@@ -198,6 +233,7 @@ int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s);
 // recon's own buffers and keeps the fastest; results are cached per geometry class (detector,
 // volume, window, interpolation and views-per-slice), so a class is tuned once per process.
 LCT_API int lct_recon_autotune(lct_recon* r, int* nz_out, int* minb_out) {
+  if (r && r->bounded) return LCT_ERR_UNSUPPORTED;  // no whole-scan buffers to time on
   if (!r) return LCT_ERR_ARG;
   const lct_geom& g = r->info.ctg;
   const lct_img& ig = r->info.ig;
@@ -210,7 +246,7 @@ LCT_API int lct_recon_autotune(lct_recon* r, int* nz_out, int* minb_out) {
   static std::map<std::vector<long long>, std::pair<int, int>> cache;
   const std::vector<long long> key = {g.ns, g.nt, ig.nx, ig.ny, g.n_angle, g.n_proj_turn,
                                       r->o.interp, (long long)(1000.0 * g.pitch / ig.dz),
-                                      (long long)r->info.n_blocks_run};
+                                      (long long)r->info.n_blocks_run, (long long)r->tex_bp};
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
@@ -229,7 +265,7 @@ LCT_API int lct_recon_autotune(lct_recon* r, int* nz_out, int* minb_out) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const size_t qbytes = sizeof(float4) * (size_t)r->g_count * quad_view_elems(g.ns, g.nt);
-  st = cuda_status(cudaMemsetAsync(r->d_quad, 0, qbytes, s));
+  if (!r->tex_bp) st = cuda_status(cudaMemsetAsync(r->d_quad, 0, qbytes, s));
   float best = 1e30f;
   int bnz = 8, bmb = 4;
   const int nzs[3] = {4, 8, 16}, mbs[3] = {2, 3, 4};
@@ -345,9 +381,9 @@ static int run_blocks(lct_recon* r, const float* d_fan, float* d_img, cudaStream
       L.nz_thread = bp_nz;
       L.minb = r->o.bp_minb;
       if (r->quads) {
-        if ((st = launch_quad_pack(r->d_par, g.n_angle, g.ns, g.nt, addr, r->d_quad, s))) return st;
+        if ((st = recon_pack(r, r->d_par, g.n_angle, 0, addr, s))) return st;
         r->launches++;
-        st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
+        st = recon_bp_pairs(r, L, s);
       } else {
         st = launch_bp_par(g, ig, L, s);
       }
@@ -395,7 +431,7 @@ int recon_stage_filter(lct_recon* r, cudaStream_t s) {
   if (r->quads && r->o.backprojector == LCT_BP_PAR) {
     // border-addressed quads; a clamped (legacy first) slab reads the FP32 views directly
     const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
-    if ((st = launch_quad_pack(r->d_par, r->g_count, g.ns, g.nt, packed, r->d_quad, s))) return st;
+    if ((st = recon_pack(r, r->d_par, r->g_count, 0, packed, s))) return st;
     r->launches++;
   }
   return LCT_OK;
@@ -423,8 +459,23 @@ void recon_bp_launch(const lct_recon* r, int b0, int b1, float* d_img, BpLaunch&
   L.betas = r->d_betas + r->g_first;
 }
 
+int recon_pack(lct_recon* r, const float* par, long long nv, long long v0, int addr, cudaStream_t s) {
+  const lct_geom& g = r->info.ctg;
+  if (r->tex_bp) return view_texture_fill(r->vtex, par, nv, v0, s);
+  if (r->quad_ring > 0)
+    return launch_quad_pack(par, nv, g.ns, g.nt, addr, r->d_quad, s, v0, r->quad_ring);
+  return launch_quad_pack(par, nv, g.ns, g.nt, addr, r->d_quad + v0 * quad_view_elems(g.ns, g.nt), s);
+}
+
+int recon_bp_pairs(lct_recon* r, BpLaunch& L, cudaStream_t s) {
+  L.quad_ring = r->quad_ring;
+  if (r->tex_bp) return launch_bp_par_texture(r->info.ctg, r->info.ig, L, r->vtex.tex, s);
+  return launch_bp_par_quads(r->info.ctg, r->info.ig, L, r->d_quad, s);
+}
+
 bool recon_bp_quads_all(const lct_recon* r) {
-  return r->quads && r->o.backprojector == LCT_BP_PAR && r->o.addr != LCT_ADDR_LEGACY;
+  return r->quads && !r->tex_bp && r->o.backprojector == LCT_BP_PAR &&
+         r->o.addr != LCT_ADDR_LEGACY;
 }
 
 int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s) {
@@ -453,7 +504,7 @@ int recon_stage_bp(lct_recon* r, float* d_img, cudaStream_t s) {
     recon_bp_launch(r, b0, b1, d_img, L);
     const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
     if (r->quads && addr == packed)
-      st = launch_bp_par_quads(g, ig, L, r->d_quad, s);
+      st = recon_bp_pairs(r, L, s);
     else
       st = launch_bp_par(g, ig, L, s);
     if (st) return st;
@@ -573,7 +624,7 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
     L.view_hi = hi;
     L.part = part;
     const int addr = block_addr(r, b);
-    const int e = (r->quads && addr == packed) ? launch_bp_par_quads(g, ig, L, r->d_quad, sb)
+    const int e = (r->quads && addr == packed) ? recon_bp_pairs(r, L, sb)
                                                : launch_bp_par(g, ig, L, sb);
     if (!e) r->launches++;
     return e;
@@ -612,9 +663,7 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
       if (st) return st;
       r->launches += filter_launches(r->o.filter_mode);
       if (r->quads) {
-        if ((st = launch_quad_pack(par, nv, g.ns, g.nt, packed,
-                                   r->d_quad + v0 * quad_view_elems(g.ns, g.nt), s)))
-          return st;
+        if ((st = recon_pack(r, par, nv, v0, packed, s))) return st;
         r->launches++;
       }
       done = target;
@@ -672,6 +721,9 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
   const int nb = r->info.n_blocks_run;
   const long long off = r->info.data_offset;
   int st;
+  if (r->bounded)  // rings: always the overlapped pipeline, from the run's first fan view
+    return recon_run_bounded_ptr(r, fan + (r->fan_first + off - fan_view0) * r->plane,
+                                 fan_on_device != 0, image, image_on_device != 0, s);
   r->launches = 0;
   r->streamed = false;
   if ((st = cuda_status(cudaEventRecord(r->ev[0], s)))) return st;
@@ -768,6 +820,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
 
 LCT_API int lct_recon_set_learned(lct_recon* r, lct_cnn* c, float bound) {
   if (!r || !(bound >= 0.f)) return LCT_ERR_ARG;
+  if (r->bounded && c) return LCT_ERR_UNSUPPORTED;  // the network reads whole-volume neighbours
   if (!c) {
     r->cnn = nullptr;
     return LCT_OK;

@@ -1,0 +1,695 @@
+// Whole-scan runs with a bounded device footprint, and runs straight from the reference's raw
+// files.
+//
+// The reference bounds device memory per 32-slice block: it reads each block's window of fan
+// views from the raw file (Src/DataReader.cpp:8-19, an `int`-sized offset), rebins, filters and
+// backprojects it, and moves on (Src/Reconstructor.cpp:33-48) -- every view is read, rebinned and
+// filtered about three times, once per block whose window holds it.  A bounded recon keeps the
+// scan-mode property (each view uploaded, rebinned and filtered once) with memory that does not
+// grow with the scan:
+//   fan    a ring of fan views: the upload of a piece overwrites only views whose rebins are done
+//   par    one piece of rebinned, filtered views (the backprojector reads the quads)
+//   quads  a ring holding the windows of the slabs in flight (quad views, or the slots of the
+//          3-D texture the TEX8 backprojector samples): a piece is packed only after every slab
+//          whose window held the slots it overwrites is backprojected
+//   img    a ring of four slabs for volumes written to host memory or a file (a device volume is
+//          written in place)
+// Slabs are taken in the order their windows end and backprojected on two alternating streams,
+// the first in parts while its window arrives, exactly as the streamed unbounded run does; the
+// kernels and their order per view are the same, so the volume is bit-identical to it.
+//
+// lct_recon_run_file reads the fan from the reference's raw file with 64-bit offsets on a reader
+// thread into pinned chunks that are uploaded as the pipeline needs them, and writes the volume
+// through a slab writer thread (64-bit offsets) -- RawDataReader::readData and RawImageWriter
+// (Src/ImageWriter.cpp:9-43) for whole scans.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <condition_variable>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "lct_internal.h"
+
+namespace lct {
+const float* plan_angles(const lct_plan* p);
+}  // namespace lct
+
+#include "recon_internal.h"
+
+namespace lct {
+
+constexpr long long kDefaultPiece = 512;  // views per rebin / filter / pack step
+constexpr int kImgRing = 4;               // slabs in the volume ring (host / file output)
+constexpr int kFanStage = 3;              // pinned fan chunks of lct_recon_run_file
+constexpr int kImgStage = 2;              // pinned slabs of the file writer
+
+// Fan views a global parallel view g reads lie in [g + lo, g + hi] (scan rebin shifts, FP64).
+static void rebin_reach(const lct_geom& g, long long& lo, long long& hi) {
+  const double s0 = ((0.0 - (double)g.ws) * (double)g.ds / (double)g.dso) / (double)g.orbit;
+  const double s1 = (((double)(g.ns - 1) - (double)g.ws) * (double)g.ds / (double)g.dso) /
+                    (double)g.orbit;
+  lo = (long long)std::floor(std::min(s0, s1));
+  hi = (long long)std::floor(std::max(s0, s1)) + 1;
+}
+
+// ----------------------------------------------------------------------------------------------
+// reader: file views -> pinned chunks (a thread), chunks -> device (the issuing thread)
+// ----------------------------------------------------------------------------------------------
+class FanReader {
+ public:
+  // views [0, nviews) of the run lie at byte0 + v * view_bytes of the file
+  int start(const char* path, long long byte0, long long view_bytes, long long nviews,
+            long long chunk, float* stage, int slots) {
+    fd_ = ::open(path, O_RDONLY);
+    if (fd_ < 0) return LCT_ERR_IO;
+    struct stat sb;
+    if (fstat(fd_, &sb) != 0 || (long long)sb.st_size < byte0 + nviews * view_bytes) {
+      ::close(fd_);
+      fd_ = -1;
+      return LCT_ERR_IO;  // the file ends before the run's last view
+    }
+    byte0_ = byte0;
+    view_bytes_ = view_bytes;
+    nviews_ = nviews;
+    chunk_ = chunk;
+    stage_ = stage;
+    slots_ = slots;
+    state_.assign(slots, kFree);
+    held_.assign(slots, -1);
+    rel_.resize(slots);
+    for (int i = 0; i < slots; ++i) rel_[i] = {this, i};
+    th_ = std::thread([this] { loop(); });
+    return LCT_OK;
+  }
+  long long chunks() const { return (nviews_ + chunk_ - 1) / chunk_; }
+  // blocks until chunk c is in its pinned slot
+  int acquire(long long c, const float** data, long long* nv) {
+    const int slot = (int)(c % slots_);
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return err_ || (state_[slot] == kReady && held_[slot] == c); });
+    if (err_) return err_;
+    *data = stage_ + (long long)slot * chunk_ * (view_bytes_ / (long long)sizeof(float));
+    *nv = std::min(chunk_, nviews_ - c * chunk_);
+    return LCT_OK;
+  }
+  // the slot of chunk c is free again once the work queued on s so far (its upload) is done
+  int release_after(cudaStream_t s, long long c) {
+    const int slot = (int)(c % slots_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      state_[slot] = kUploading;
+    }
+    return cuda_status(cudaLaunchHostFunc(s, &FanReader::on_uploaded, &rel_[slot]));
+  }
+  // stops the thread (every queued upload must have completed); the first error, if any
+  int finish() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (th_.joinable()) th_.join();
+    if (fd_ >= 0) ::close(fd_);
+    fd_ = -1;
+    return err_;
+  }
+
+ private:
+  enum { kFree = 0, kReading = 1, kReady = 2, kUploading = 3 };
+  struct Rel {
+    FanReader* self;
+    int slot;
+  };
+  static void CUDART_CB on_uploaded(void* p) {  // a CUDA host function: no CUDA calls here
+    Rel* r = static_cast<Rel*>(p);
+    {
+      std::lock_guard<std::mutex> lk(r->self->mu_);
+      r->self->state_[r->slot] = kFree;
+    }
+    r->self->cv_.notify_all();
+  }
+  void loop() {
+    for (long long c = 0; c < chunks(); ++c) {
+      const int slot = (int)(c % slots_);
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || state_[slot] == kFree; });
+        if (stop_) return;
+        state_[slot] = kReading;
+      }
+      const long long nv = std::min(chunk_, nviews_ - c * chunk_);
+      char* dst = reinterpret_cast<char*>(stage_) + (long long)slot * chunk_ * view_bytes_;
+      long long left = nv * view_bytes_, off = byte0_ + c * chunk_ * view_bytes_;
+      int e = LCT_OK;
+      while (left > 0) {
+        const ssize_t n = ::pread(fd_, dst, (size_t)std::min<long long>(left, 1LL << 30), (off_t)off);
+        if (n < 0 && errno == EINTR) continue;
+        if (n <= 0) {
+          e = LCT_ERR_IO;
+          break;
+        }
+        dst += n;
+        off += n;
+        left -= n;
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (e) err_ = e;
+        held_[slot] = c;
+        state_[slot] = kReady;
+      }
+      cv_.notify_all();
+      if (e) return;
+    }
+  }
+  int fd_ = -1;
+  long long byte0_ = 0, view_bytes_ = 0, nviews_ = 0, chunk_ = 1;
+  float* stage_ = nullptr;
+  int slots_ = 0;
+  std::vector<int> state_;
+  std::vector<long long> held_;
+  std::vector<Rel> rel_;
+  std::thread th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  bool stop_ = false;
+  int err_ = LCT_OK;
+};
+
+// ----------------------------------------------------------------------------------------------
+// writer: device slab -> pinned slot (D2H on the download stream) -> file (a thread)
+// ----------------------------------------------------------------------------------------------
+class SlabWriter {
+ public:
+  int start(const char* path, long long slab_bytes, int nslabs, float* stage, int slots) {
+    fd_ = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd_ < 0) return LCT_ERR_IO;
+    if (::ftruncate(fd_, (off_t)(slab_bytes * nslabs)) != 0) {
+      ::close(fd_);
+      fd_ = -1;
+      return LCT_ERR_IO;
+    }
+    slab_bytes_ = slab_bytes;
+    stage_ = stage;
+    slots_ = slots;
+    busy_.assign(slots, 0);
+    dest_.assign(slots, -1);
+    sub_.resize(slots);
+    for (int i = 0; i < slots; ++i) sub_[i] = {this, i};
+    th_ = std::thread([this] { loop(); });
+    return LCT_OK;
+  }
+  // pinned slot for the k-th slab written (blocks while its previous slab is being written)
+  int slot_for(int k, float** p) {
+    const int slot = k % slots_;
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return err_ || !busy_[slot]; });
+    if (err_) return err_;
+    busy_[slot] = 1;
+    *p = stage_ + (long long)slot * (slab_bytes_ / (long long)sizeof(float));
+    return LCT_OK;
+  }
+  // once the work queued on s (the slab's download into slot k % slots) is done, write it as
+  // slab `dest` of the file
+  int submit_after(cudaStream_t s, int k, int dest) {
+    const int slot = k % slots_;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      dest_[slot] = dest;
+    }
+    return cuda_status(cudaLaunchHostFunc(s, &SlabWriter::on_downloaded, &sub_[slot]));
+  }
+  int finish() {
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      cv_.wait(lk, [&] {
+        if (err_) return true;
+        for (int b : busy_)
+          if (b) return false;
+        return true;
+      });
+      stop_ = true;
+    }
+    cv_.notify_all();
+    if (th_.joinable()) th_.join();
+    if (fd_ >= 0 && ::close(fd_) != 0 && !err_) err_ = LCT_ERR_IO;
+    fd_ = -1;
+    return err_;
+  }
+
+ private:
+  struct Sub {
+    SlabWriter* self;
+    int slot;
+  };
+  static void CUDART_CB on_downloaded(void* p) {  // a CUDA host function: no CUDA calls here
+    Sub* s = static_cast<Sub*>(p);
+    {
+      std::lock_guard<std::mutex> lk(s->self->mu_);
+      s->self->ready_.push_back(s->slot);
+    }
+    s->self->cv_.notify_all();
+  }
+  void loop() {
+    for (;;) {
+      int slot;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return stop_ || !ready_.empty(); });
+        if (ready_.empty()) return;
+        slot = ready_.front();
+        ready_.erase(ready_.begin());
+      }
+      const char* src = reinterpret_cast<const char*>(stage_) + (long long)slot * slab_bytes_;
+      long long left = slab_bytes_, off = (long long)dest_[slot] * slab_bytes_;
+      int e = LCT_OK;
+      while (left > 0) {
+        const ssize_t n = ::pwrite(fd_, src, (size_t)std::min<long long>(left, 1LL << 30), (off_t)off);
+        if (n < 0 && errno == EINTR) continue;
+        if (n <= 0) {
+          e = LCT_ERR_IO;
+          break;
+        }
+        src += n;
+        off += n;
+        left -= n;
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (e && !err_) err_ = e;
+        busy_[slot] = 0;
+      }
+      cv_.notify_all();
+    }
+  }
+  int fd_ = -1;
+  long long slab_bytes_ = 0;
+  float* stage_ = nullptr;
+  int slots_ = 0;
+  std::vector<int> busy_, dest_, ready_;
+  std::vector<Sub> sub_;
+  std::thread th_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  bool stop_ = false;
+  int err_ = LCT_OK;
+};
+
+// ----------------------------------------------------------------------------------------------
+// the pipeline
+// ----------------------------------------------------------------------------------------------
+struct FanFeed {
+  const float* dev = nullptr;   // device fan, the run's view 0 (read in place)
+  const float* host = nullptr;  // host fan, the run's view 0
+  FanReader* reader = nullptr;  // file
+};
+struct ImageSink {
+  float* dev = nullptr;         // the caller's device volume (written in place)
+  float* host = nullptr;        // the caller's host volume
+  SlabWriter* writer = nullptr;  // a file
+};
+
+// Events of one run: 5 for the fork and join, per slab: views ready, backprojected, downloaded;
+// per piece: uploaded, packed.
+static int run_events(lct_recon* r, long long n_pieces, cudaEvent_t** base) {
+  const int nb = r->info.n_blocks_run;
+  const size_t n_ev = 5 + 3 * (size_t)nb + 2 * (size_t)n_pieces;
+  while (r->sev.size() < n_ev) {
+    cudaEvent_t e;
+    int st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (st) return st;
+    r->sev.push_back(e);
+  }
+  *base = r->sev.data();
+  return LCT_OK;
+}
+
+static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink, cudaStream_t s,
+                        const StreamSet& ss) {
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  const int nb = r->info.n_blocks_run;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  const long long plane = r->plane;
+  const long long P = r->piece > 0 ? r->piece : kDefaultPiece;
+  int st;
+  const long long n_pieces = r->g_count / P + nb + 1;
+  cudaEvent_t* ev = nullptr;
+  if ((st = run_events(r, n_pieces, &ev))) return st;
+  cudaEvent_t* ev_views = ev + 5;
+  cudaEvent_t* ev_bp = ev_views + nb;
+  cudaEvent_t* ev_dl = ev_bp + nb;
+  cudaEvent_t* ev_up = ev_dl + nb;
+  cudaEvent_t* ev_packed = ev_up + n_pieces;
+  long long piece = 0;
+
+  long long reach_lo, reach_hi;
+  rebin_reach(g, reach_lo, reach_hi);
+  std::vector<int> order(nb);
+  std::vector<long long> gfirst(nb), gend(nb);
+  for (int b = 0; b < nb; ++b) {
+    order[b] = b;
+    gfirst[b] = r->blocks[b].block_proj_start + g.add_projections;
+    gend[b] = gfirst[b] + g.n_angle;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return gend[x] < gend[y]; });
+  const int packed = r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  const long long fan_ring = feed.dev ? 0 : r->fan_ring;
+  long long done = r->g_first, up = 0;  // global views packed so far; fan views uploaded
+  int waited = 0;                       // slabs (in processing order) the packs have waited for
+  const bool ring_img = !sink.dev && r->img_ring > 0;
+  float* const img_base = sink.dev ? sink.dev : r->d_img;
+
+  // fan views [a, b) of the run into the fan buffer (a ring: split at its end)
+  auto upload = [&](long long a, long long b, const float* src) -> int {
+    while (a < b) {
+      const long long slot = fan_ring > 0 ? a % fan_ring : a;
+      const long long n = fan_ring > 0 ? std::min(b - a, fan_ring - slot) : b - a;
+      int e = cuda_status(cudaMemcpyAsync(r->d_fan + slot * plane, src, sizeof(float) * n * plane,
+                                          cudaMemcpyHostToDevice, ss.up));
+      if (e) return e;
+      a += n;
+      src += n * plane;
+    }
+    return LCT_OK;
+  };
+  auto bp = [&](int k, int b, int lo, int hi, int part, cudaStream_t sb) -> int {
+    BpLaunch L;
+    recon_bp_launch(r, b, b + 1, img_base, L);
+    if (ring_img) {
+      L.img = r->d_img + (long long)(k % r->img_ring) * slab;
+      L.slab_z0[0] = 0;
+    }
+    L.view_lo = lo;
+    L.view_hi = hi;
+    L.part = part;
+    const int e = recon_bp_pairs(r, L, sb);
+    if (!e) r->launches++;
+    return e;
+  };
+  for (int k = 0; k < nb; ++k) {
+    const int b = order[k];
+    cudaStream_t sb = ss.bp[k & 1];
+    const bool split = k == 0;  // the first slab in parts as its views arrive
+    const long long slab_end = std::min(gend[b], r->g_first + r->g_count);
+    int bp_lo = 0, parts = 0;
+    while (slab_end > done) {
+      const long long target = std::min(slab_end, done + P);
+      const long long need = std::min(r->fan_count, target + reach_hi + 1 - r->fan_first);
+      if (piece >= n_pieces) return LCT_ERR_ARG;  // cannot happen: pieces are counted above
+      if (!feed.dev && need > up) {
+        // the upload overwrites ring slots of views only the rebins up to piece - 2 read
+        if (fan_ring > 0 && piece >= 2 &&
+            (st = cuda_status(cudaStreamWaitEvent(ss.up, ev_packed[piece - 2], 0))))
+          return st;
+        if (feed.reader) {
+          while (up < need) {  // whole chunks, in order
+            const float* h = nullptr;
+            long long nv = 0;
+            if ((st = feed.reader->acquire(up / P, &h, &nv))) return st;
+            if ((st = upload(up, up + nv, h))) return st;
+            if ((st = feed.reader->release_after(ss.up, up / P))) return st;
+            up += nv;
+          }
+        } else {
+          if ((st = upload(up, need, feed.host + up * plane))) return st;
+          up = need;
+        }
+      }
+      if ((st = cuda_status(cudaEventRecord(ev_up[piece], ss.up)))) return st;
+      if ((st = cuda_status(cudaStreamWaitEvent(s, ev_up[piece], 0)))) return st;
+      // the pack overwrites quad-ring slots of views [target - ring - (target - done), target -
+      // ring): wait for every slab whose window holds one of them
+      if (r->quad_ring > 0) {
+        while (waited < k && gfirst[order[waited]] < target - r->quad_ring) {
+          if ((st = cuda_status(cudaStreamWaitEvent(s, ev_bp[waited], 0)))) return st;
+          ++waited;
+        }
+        if (waited < nb && waited >= k && k < nb && gfirst[order[waited]] < target - r->quad_ring)
+          return LCT_ERR_UNSUPPORTED;  // a slab not yet backprojected would lose views (ring too small)
+      }
+      const long long v0 = done - r->g_first, nv = target - done;
+      float* par = r->bounded ? r->d_par : r->d_par + v0 * plane;
+      if ((st = launch_rebin_fan2par_scan(g, feed.dev ? feed.dev : r->d_fan, r->fan_first,
+                                          r->fan_count, par, done, nv, r->o.interp, packed, s,
+                                          fan_ring)))
+        return st;
+      r->launches++;
+      if (r->o.filter_mode != LCT_FILTER_FP32)
+        st = tc_filter(g.ns, par, nv * g.nt, r->d_tc, r->tc_rows, r->o.filter_mode, s);
+      else
+        st = launch_filter_rows(g.ns, r->d_h, par, nv * g.nt, LCT_FILTER_FP32, s);
+      if (st) return st;
+      r->launches += filter_launches(r->o.filter_mode);
+      if ((st = recon_pack(r, par, nv, v0, packed, s))) return st;
+      r->launches++;
+      done = target;
+      if ((st = cuda_status(cudaEventRecord(ev_packed[piece], s)))) return st;
+      ++piece;
+      // a pair starting at local view ia also reads its conjugate ia + half: a part takes the
+      // pair starts whose conjugates are packed too
+      const long long local = std::min<long long>(done - gfirst[b], g.n_angle);
+      const int avail = (int)std::max<long long>(local - g.n_proj_turn / 2, 0);
+      if (split && done < slab_end && avail > bp_lo) {
+        if ((st = cuda_status(cudaStreamWaitEvent(sb, ev_packed[piece - 1], 0)))) return st;
+        if ((st = bp(k, b, bp_lo, avail, parts ? kBpMiddle : kBpFirst, sb))) return st;
+        bp_lo = avail;
+        ++parts;
+      }
+    }
+    if ((st = cuda_status(cudaEventRecord(ev_views[k], s)))) return st;
+    if ((st = cuda_status(cudaStreamWaitEvent(sb, ev_views[k], 0)))) return st;
+    // the volume slot is free once the slab that used it before is downloaded
+    if (ring_img && k >= r->img_ring &&
+        (st = cuda_status(cudaStreamWaitEvent(sb, ev_dl[k - r->img_ring], 0))))
+      return st;
+    if ((st = parts ? bp(k, b, bp_lo, g.n_angle, kBpLast, sb) : bp(k, b, 0, 1 << 30, kBpWhole, sb)))
+      return st;
+    if ((st = cuda_status(cudaEventRecord(ev_bp[k], sb)))) return st;
+    const float* src = ring_img ? r->d_img + (long long)(k % r->img_ring) * slab
+                                : img_base + (long long)b * slab;
+    if (sink.host || sink.writer) {
+      if ((st = cuda_status(cudaStreamWaitEvent(ss.down, ev_bp[k], 0)))) return st;
+      float* dst = sink.host ? sink.host + (long long)b * slab : nullptr;
+      if (sink.writer && (st = sink.writer->slot_for(k, &dst))) return st;
+      if ((st = cuda_status(cudaMemcpyAsync(dst, src, sizeof(float) * slab, cudaMemcpyDeviceToHost,
+                                            ss.down))))
+        return st;
+      if (sink.writer && (st = sink.writer->submit_after(ss.down, k, b))) return st;
+    }
+    if ((st = cuda_status(cudaEventRecord(ev_dl[k], sink.host || sink.writer ? ss.down : sb))))
+      return st;
+  }
+  return LCT_OK;
+}
+
+// Fork the streams from s, run, join them back and time the span; on an error every stream is
+// drained before returning (host functions of the reader and writer may still be queued).
+template <class F>
+static int run_forked(lct_recon* r, cudaStream_t s, F body) {
+  int st;
+  r->launches = 0;
+  r->streamed = true;
+  if ((st = cuda_status(cudaEventRecord(r->ev[0], s)))) return st;
+  for (int i = 1; i < 4; ++i)
+    if ((st = cuda_status(cudaEventRecord(r->ev[i], s)))) return st;
+  if ((st = streams_create(r->ss))) return st;
+  cudaEvent_t* ev = nullptr;
+  if ((st = run_events(r, 0, &ev))) return st;
+  if ((st = streams_fork(r->ss, s, r->sev[0]))) return st;
+  st = body();
+  int st2 = streams_join(r->ss, s, r->sev.data() + 1);
+  if (st) {
+    cudaStream_t all[5] = {r->ss.up, r->ss.down, r->ss.bp[0], r->ss.bp[1], s};
+    for (cudaStream_t x : all) cudaStreamSynchronize(x);
+    return st;
+  }
+  if (st2) return st2;
+  if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
+  if ((st = cuda_status(cudaEventRecord(r->ev[5], s)))) return st;
+  if ((st = cuda_status(cudaEventSynchronize(r->ev[5])))) return st;
+  for (int i = 0; i < 5; ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r->ev[i], r->ev[i + 1]);
+    r->times[i] = ms;
+  }
+  r->cnn_ms = 0.f;
+  return LCT_OK;
+}
+
+int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, float* image,
+                          bool image_on_device, cudaStream_t s) {
+  FanFeed feed;
+  ImageSink sink;
+  if (fan_on_device)
+    feed.dev = fan;
+  else
+    feed.host = fan;
+  if (image_on_device)
+    sink.dev = image;
+  else
+    sink.host = image;
+  return run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
+}
+
+void recon_free_bounded(lct_recon* r) {
+  if (r->h_fan_stage) cudaFreeHost(r->h_fan_stage);
+  if (r->h_img_stage) cudaFreeHost(r->h_img_stage);
+  r->h_fan_stage = r->h_img_stage = nullptr;
+}
+
+}  // namespace lct
+
+using namespace lct;
+
+LCT_API int lct_recon_create_bounded(const lct_plan* plan, const lct_recon_opts* opts,
+                                     int piece_views, lct_recon** out) {
+  if (piece_views < 0) return LCT_ERR_ARG;
+  lct_recon* r = nullptr;
+  int st = recon_setup(plan, opts, &r);
+  if (st) return st;
+  const lct_geom& g = r->info.ctg;
+  const lct_img& ig = r->info.ig;
+  const int nb = r->info.n_blocks_run;
+  if (!recon_streamable(r) || !r->quads || r->o.addr == LCT_ADDR_LEGACY) {
+    lct_recon_destroy(r);
+    return LCT_ERR_UNSUPPORTED;
+  }
+  if (r->o.bp_nz == -1) r->o.bp_nz = 0;  // no whole-scan buffers to tune on: the default shape
+  r->bounded = true;
+  r->piece = piece_views > 0 ? piece_views : kDefaultPiece;
+  const long long P = r->piece;
+  long long reach_lo, reach_hi;
+  rebin_reach(g, reach_lo, reach_hi);
+  // fan ring: the views the rebins of two consecutive pieces read, plus a chunk of read-ahead
+  const long long fr = 3 * P + (reach_hi - reach_lo) + 16;
+  r->fan_ring = fr < r->fan_count ? fr : 0;
+  // quad ring: a window, a piece and the two slab strides the alternating streams keep in flight
+  long long stride = 0;
+  for (int b = 1; b < nb; ++b)
+    stride = std::max<long long>(stride, std::llabs((long long)r->blocks[b].block_proj_start -
+                                                   r->blocks[b - 1].block_proj_start));
+  const long long qr = g.n_angle + P + 2 * stride + 16;
+  r->quad_ring = qr < r->g_count ? qr : 0;
+  r->img_ring = nb > kImgRing ? kImgRing : 0;
+  const long long fan_views = r->fan_ring > 0 ? r->fan_ring : r->fan_count;
+  const long long quad_views = r->quad_ring > 0 ? r->quad_ring : r->g_count;
+  const long long img_slabs = r->img_ring > 0 ? r->img_ring : nb;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  auto alloc = [&](void** p, size_t bytes) {
+    int e = cuda_status(cudaMalloc(p, bytes));
+    if (!e) r->device_bytes += (long long)bytes;
+    return e;
+  };
+  do {
+    if ((st = alloc((void**)&r->d_fan, sizeof(float) * fan_views * r->plane))) break;
+    if ((st = alloc((void**)&r->d_par, sizeof(float) * P * r->plane))) break;
+    if ((st = alloc((void**)&r->d_img, sizeof(float) * img_slabs * slab))) break;
+    if (r->tex_bp) {
+      if ((st = view_texture_create(r->vtex, g.ns, g.nt, quad_views,
+                                    r->o.addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER))) {
+        if (st != LCT_ERR_UNSUPPORTED) break;
+        r->tex_bp = false;  // deeper than the device's 3-D texture limit: quads
+        st = LCT_OK;
+      } else {
+        r->device_bytes += (long long)sizeof(float) * quad_views * r->plane;
+      }
+    }
+    if (!r->tex_bp &&
+        (st = alloc((void**)&r->d_quad, sizeof(float4) * quad_views * quad_view_elems(g.ns, g.nt))))
+      break;
+    if (r->o.filter_mode != LCT_FILTER_FP32) r->tc_rows = P * g.nt;
+    st = recon_alloc_common(r, plan);
+  } while (0);
+  if (st) {
+    lct_recon_destroy(r);
+    return recon_alloc_status(st);
+  }
+  *out = r;
+  return LCT_OK;
+}
+
+LCT_API int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes) {
+  if (!r || !bytes) return LCT_ERR_ARG;
+  *bytes = r->device_bytes;
+  return LCT_OK;
+}
+
+LCT_API int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path,
+                               float* image, lct_stream stream) {
+  if (!r || !fan_path || (!image_path && !image)) return LCT_ERR_ARG;
+  if (!recon_streamable(r) || !r->quads || r->o.addr == LCT_ADDR_LEGACY) return LCT_ERR_UNSUPPORTED;
+  if (r->cnn) return LCT_ERR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  const lct_img& ig = r->info.ig;
+  const int nb = r->info.n_blocks_run;
+  const long long P = r->piece > 0 ? r->piece : kDefaultPiece;
+  const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+  int st;
+  // pinned staging, allocated on the first call and kept with the recon
+  if (!r->h_fan_stage) {
+    if ((st = cuda_status(cudaHostAlloc((void**)&r->h_fan_stage,
+                                        sizeof(float) * kFanStage * P * r->plane,
+                                        cudaHostAllocDefault))))
+      return recon_alloc_status(st);
+    r->fan_stage_slots = kFanStage;
+  }
+  if (image_path && !r->h_img_stage) {
+    if ((st = cuda_status(cudaHostAlloc((void**)&r->h_img_stage, sizeof(float) * kImgStage * slab,
+                                        cudaHostAllocDefault))))
+      return recon_alloc_status(st);
+    r->img_stage_slots = kImgStage;
+  }
+  FanReader reader;
+  SlabWriter writer;
+  // file view v of the run's fan views lies at (fan_first + DataOffset + v) views into the file
+  // (Src/DataReader.cpp:14, in 64 bits)
+  const long long view_bytes = (long long)sizeof(float) * r->plane;
+  const long long byte0 = (r->fan_first + r->info.data_offset) * view_bytes;
+  if ((st = reader.start(fan_path, byte0, view_bytes, r->fan_count, P, r->h_fan_stage,
+                         r->fan_stage_slots)))
+    return st;
+  if (image_path && (st = writer.start(image_path, (long long)sizeof(float) * slab, nb,
+                                       r->h_img_stage, r->img_stage_slots))) {
+    reader.finish();
+    return st;
+  }
+  FanFeed feed;
+  feed.reader = &reader;
+  ImageSink sink;
+  sink.host = image;
+  sink.writer = image_path ? &writer : nullptr;
+  if (image && image_path) {
+    // one download per slab: the file is written from the caller's buffer's copy as well
+    sink.host = nullptr;
+  }
+  st = run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
+  const int st_r = reader.finish();
+  const int st_w = image_path ? writer.finish() : LCT_OK;
+  if (!st && image && image_path) {
+    // the caller also wants the volume in memory: read back what the writer wrote
+    const int fd = ::open(image_path, O_RDONLY);
+    if (fd < 0) return LCT_ERR_IO;
+    char* dst = reinterpret_cast<char*>(image);
+    long long left = (long long)sizeof(float) * slab * nb, off = 0;
+    while (left > 0) {
+      const ssize_t n = ::pread(fd, dst, (size_t)std::min<long long>(left, 1LL << 30), (off_t)off);
+      if (n <= 0) {
+        ::close(fd);
+        return LCT_ERR_IO;
+      }
+      dst += n;
+      off += n;
+      left -= n;
+    }
+    ::close(fd);
+  }
+  return st ? st : (st_r ? st_r : st_w);
+}

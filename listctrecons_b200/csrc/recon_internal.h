@@ -33,7 +33,9 @@ struct lct_recon {
   float4* d_quad = nullptr;  // filtered views in quad layout (backprojection input)
   void* d_tc = nullptr;      // BF16x3 filter operands (row and Toeplitz planes)
   long long tc_rows = 0;
-  bool quads = false;        // full windows: the quad-layout pairs kernel applies
+  bool quads = false;        // full windows: the pairs kernels (quads or texture) apply
+  bool tex_bp = false;       // the pairs backprojection samples a 3-D texture (TEX8) instead
+  lct::ViewTexture vtex;     // filtered views as that texture (scan: global views; block: one block)
   cudaEvent_t ev[6] = {};
   float times[5] = {};
   lct_cnn* cnn = nullptr;    // learned correction after backprojection (not owned)
@@ -48,9 +50,54 @@ struct lct_recon {
   int device = 0;
   long long voxel_updates = 0;
   int launches = 0;
+  // bounded device memory (lct_recon_create_bounded): d_fan, d_quad and d_img are rings and
+  // d_par / d_tc hold one piece; 0 rings mean whole buffers
+  bool bounded = false;
+  long long piece = 0;       // views rebinned, filtered and packed per step
+  long long fan_ring = 0;    // fan views in d_fan (0: fan_count, linear)
+  long long quad_ring = 0;   // views in d_quad (0: g_count, linear)
+  int img_ring = 0;          // slabs in d_img for host / file output (0: the whole volume)
+  long long device_bytes = 0;
+  // pinned host staging of lct_recon_run_file (allocated on its first call, kept until destroy)
+  float* h_fan_stage = nullptr;
+  float* h_img_stage = nullptr;
+  int fan_stage_slots = 0, img_stage_slots = 0;
 };
 
 namespace lct {
+// backprojection slices per thread: the requested 4 / 8 / 16, else the measured default (8,
+// or 4 when a view stays active for fewer than 6 slices: (feed / 2) / dz)
+inline int pick_bp_nz(const lct_geom& g, const lct_img& ig, int requested) {
+  if (requested == 4 || requested == 8 || requested == 16) return requested;
+  const double act = 0.5 * (double)g.pitch / (double)ig.dz;
+  return act < 6.0 ? 4 : 8;
+}
+// kernels one filter call launches
+inline int filter_launches(int mode) { return mode == LCT_FILTER_FP32 ? 1 : 2; }
+// addressing of block b (LEGACY: clamped first block, border afterwards)
+inline int block_addr(const lct_recon* r, int b) {
+  if (r->o.addr == LCT_ADDR_LEGACY) return b == 0 ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  return r->o.addr;
+}
+
+// creation steps shared by lct_recon_create and lct_recon_create_bounded (recon.cu)
+int recon_setup(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** out);
+int recon_alloc_common(lct_recon* r, const lct_plan* plan);
+int recon_alloc_status(int st);
+
+// the sampler a recon's options select: texture for TEX8 (AUTO or TEXTURE) when the windows
+// are full and the addressing is one mode for every slab; else quads
+inline bool want_texture(const lct_recon_opts& o, bool full_windows) {
+  return full_windows && o.backprojector == LCT_BP_PAR && o.interp == LCT_INTERP_TEX8 &&
+         o.addr != LCT_ADDR_LEGACY &&
+         (o.bp_sampler == LCT_BP_SAMPLER_AUTO || o.bp_sampler == LCT_BP_SAMPLER_TEXTURE);
+}
+// the filtered views [v0, v0 + nv) (at par) into the backprojector's input: texture slots or
+// quads, ring-aware (bounded recons)
+int recon_pack(lct_recon* r, const float* par, long long nv, long long v0, int addr, cudaStream_t s);
+// one pairs backprojection launch (quads or texture)
+int recon_bp_pairs(lct_recon* r, BpLaunch& L, cudaStream_t s);
+
 // scan-mode stages of one recon, on any stream (used by lct_recon_run and the batch graphs)
 int recon_stage_rebin(lct_recon* r, const float* d_fan, cudaStream_t s);
 int recon_stage_filter(lct_recon* r, cudaStream_t s);
@@ -62,6 +109,11 @@ bool recon_bp_quads_all(const lct_recon* r);
 bool recon_streamable(const lct_recon* r);
 int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, float* d_img,
                        float* d_out, float* image_host, cudaStream_t s, const StreamSet& ss);
+// Runs of a bounded recon (recon_bounded.cu): fan from a host or device pointer (fan points at
+// the run's first view), volume to a device or host pointer.
+int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, float* image,
+                          bool image_on_device, cudaStream_t s);
+void recon_free_bounded(lct_recon* r);  // pinned staging of lct_recon_run_file
 // learned correction of slices [z0, z1) of an nz-slice volume (cnn.cu)
 int cnn_infer_range(lct_cnn* c, const float* d_vol, float* d_out, int nz, int z0, int z1,
                     float bound, cudaStream_t s);

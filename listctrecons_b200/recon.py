@@ -93,15 +93,25 @@ def recon_opts(**kw) -> capi.ReconOpts:
 
 class Reconstruction:
     """lct_recon: device buffers sized from the plan, allocated once; run() reconstructs
-    n_blocks_run blocks from host or device fan projections of the whole scan."""
+    n_blocks_run blocks from host or device fan projections of the whole scan.
 
-    def __init__(self, plan: Plan, **opts):
+    bounded=True: lct_recon_create_bounded -- fan, filtered and quad views in rings sized to the
+    slab windows in flight and a four-slab volume ring for host output, so the device footprint
+    does not grow with the scan (piece_views: views per rebin/filter/pack step, 0 = default)."""
+
+    def __init__(self, plan: Plan, bounded: bool = False, piece_views: int = 0, **opts):
         self._lib = capi.load()
         self.plan = plan
+        self.bounded = bounded
         self.opts = recon_opts(**opts)
         h = C.c_void_p()
-        capi.check(self._lib.lct_recon_create(plan.handle, C.byref(self.opts), C.byref(h)),
-                   "lct_recon_create")
+        if bounded:
+            capi.check(self._lib.lct_recon_create_bounded(plan.handle, C.byref(self.opts),
+                                                          int(piece_views), C.byref(h)),
+                       "lct_recon_create_bounded")
+        else:
+            capi.check(self._lib.lct_recon_create(plan.handle, C.byref(self.opts), C.byref(h)),
+                       "lct_recon_create")
         self._h = h
         first, count = C.c_int64(), C.c_int64()
         capi.check(self._lib.lct_recon_fan_range(h, C.byref(first), C.byref(count)))
@@ -127,6 +137,30 @@ class Reconstruction:
         capi.check(self._lib.lct_recon_run(self._h, f_ptr, int(fan_view0), int(f_dev), i_ptr,
                                            int(i_dev), s), "lct_recon_run")
         return image
+
+    def run_file(self, fan_path, image_path=None, image=None, stream=None):
+        """lct_recon_run_file: the fan read from the reference's raw file (view v at byte
+        (v + DataOffset) * nt * ns * 4), the volume written to image_path and/or the host array
+        `image` (C-contiguous float32 of image_shape).  Returns `image`."""
+        if image_path is None and image is None:
+            raise ValueError("give image_path, image or both")
+        ip = None
+        if image is not None:
+            on_dev, ip = _ptr(image)
+            if on_dev:
+                raise ValueError("run_file writes a host volume")
+            if int(np.prod(image.shape)) < int(np.prod(self.image_shape)):
+                raise ValueError(f"image smaller than {self.image_shape}")
+        s = stream if stream is not None else _stream()
+        capi.check(self._lib.lct_recon_run_file(
+            self._h, str(fan_path).encode(), None if image_path is None else str(image_path).encode(),
+            ip, s), "lct_recon_run_file")
+        return image
+
+    def device_bytes(self) -> int:
+        n = C.c_int64()
+        capi.check(self._lib.lct_recon_device_bytes(self._h, C.byref(n)))
+        return n.value
 
     def stats(self) -> capi.ReconStats:
         st = capi.ReconStats()

@@ -58,3 +58,13 @@ def test_simulator_and_voxeliser_reject_bad_arguments():
                                None) == capi.LCT_ERR_ARG
     assert lib.lct_sim_project(p, 1, 8, 2, 0.0, 1.0, 3.5, 0.5, 570.0, p, p, 0, 4, 1e5, 1, p,
                                None) == capi.LCT_ERR_ARG
+
+
+def test_bounded_and_file_runs_reject_bad_arguments():
+    lib = capi.load()
+    h = C.c_void_p()
+    assert lib.lct_recon_create_bounded(None, None, 0, C.byref(h)) == capi.LCT_ERR_ARG
+    assert lib.lct_recon_create_bounded(None, None, -1, C.byref(h)) == capi.LCT_ERR_ARG
+    n = C.c_int64()
+    assert lib.lct_recon_device_bytes(None, C.byref(n)) == capi.LCT_ERR_ARG
+    assert lib.lct_recon_run_file(None, b"x", b"y", None, None) == capi.LCT_ERR_ARG

@@ -45,3 +45,79 @@ def test_dropin_matches_reference_program(cuda, tmp_path, filt):
     print(f"drop-in ({filt}) vs reference program: image rel_l2={err:.3e}, filtered {errf:.3e}")
     assert a.size == b.size and err < 1e-4
     assert errf < 1e-5
+
+
+TYPED = ROOT / "listctrecons_b200" / "dropin" / "_build" / "LISTCTRecons_b200"
+
+
+def _typed_run(prm_src: Path, out_dir: Path, rtype: str, env_extra: dict) -> tuple[np.ndarray, dict]:
+    """LISTCTRecons_b200 on a copy of prm_src writing to out_dir; (image, its JSON record)."""
+    import json
+
+    out_dir.mkdir()
+    txt = prm_src.read_text()
+    for line in txt.splitlines():
+        if line.startswith("OutputDir:"):
+            txt = txt.replace(line, f"OutputDir: {out_dir}/")
+    prm = out_dir / "scan.prm"
+    prm.write_text(txt)
+    env = dict(os.environ, **env_extra)
+    d = subprocess.run([str(TYPED), str(prm), rtype], capture_output=True, text=True, timeout=900,
+                       env=env)
+    assert d.returncode == 0, d.stdout[-1500:]
+    assert "[ERROR]" not in d.stdout, d.stdout[-1500:]
+    rec = json.loads(d.stdout.strip().splitlines()[-1])
+    return np.fromfile(out_dir / "image.raw", dtype=np.float32), rec
+
+
+@pytest.mark.skipif(not (TYPED.exists() and REF.exists()), reason="builds need the reference tree")
+def test_factory_types_through_the_reference_interfaces(cuda, tmp_path):
+    """The typed drop-in program builds its reconstructor with the reference's factory call
+    (ReconstrctorAbstractFactory::createReconstructor) and runs Reconstructor::reconstruct:
+      * "Helicalfdkramprebingpu" -- the drop-in stages, per block -- matches the reference
+        program built from its own sources (rel-L2 < 1e-4);
+      * "Helicalfdkramprebinb200" -- the whole-scan path, every view read once from the raw file
+        with 64-bit offsets -- in the reference's sampling (TEX8, FP32 filter, its legacy
+        first-block addressing) matches the reference program (rel-L2 < 1e-4), and in its default
+        mode (exact, BF16x6, bounded memory) matches the FP64 oracle (rel-L2 < 1e-4)."""
+    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.scan import write_scan_files
+    from tests.golden.make_gpu_golden import small_scan
+
+    geo, _, fan = small_scan()
+    prm = write_scan_files(geo, fan, tmp_path / "data", tmp_path / "ref")
+    r = subprocess.run([str(REF), str(prm)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-1500:]
+    ref = np.fromfile(tmp_path / "ref" / "image.raw", dtype=np.float32)
+
+    stages, rec = _typed_run(prm, tmp_path / "stages", "Helicalfdkramprebingpu",
+                             {"LCT_DROPIN_FILTER": "fp32"})
+    assert rec["type"] == "Helicalfdkramprebingpu"
+    err = orc.rel_l2(stages, ref)
+    print(f"typed program, reference type vs reference program: rel_l2={err:.3e}")
+    assert stages.size == ref.size and err < 1e-4
+
+    same, _ = _typed_run(prm, tmp_path / "b200_ref_sampling", "Helicalfdkramprebinb200",
+                         {"LCT_DROPIN_INTERP": "tex8", "LCT_DROPIN_FILTER": "fp32",
+                          "LCT_DROPIN_ADDR": "legacy"})
+    err = orc.rel_l2(same, ref)
+    print(f"whole-scan type (tex8, fp32, legacy) vs reference program: rel_l2={err:.3e}")
+    assert same.size == ref.size and err < 1e-4
+
+    fast, _ = _typed_run(prm, tmp_path / "b200", "Helicalfdkramprebinb200", {})
+    p = Plan(geo)
+    g, ig = p.info.ctg, p.info.ig
+    h = orc.ramp_taps(g.ns, g.ds)
+    vols = []
+    for b in range(p.info.n_blocks):
+        bi = p.blocks[b]
+        blk = fan[bi.block_proj_start: bi.block_proj_start + g.n_angle_add]
+        par = orc.rebin_fan2par(g, blk, orc.EXACT).astype(np.float32)
+        f = orc.filter_rows_fp64(h, par).astype(np.float32)
+        betas = p.angles32[bi.block_proj_start + g.add_projections:][: g.n_angle]
+        vols.append(orc.bp_par_cols(g, ig, betas, f, orc.EXACT))
+    oracle = np.concatenate(vols, 0).ravel()
+    err = orc.rel_l2(fast, oracle)
+    print(f"whole-scan type (exact, bf16x6, bounded) vs FP64 oracle: rel_l2={err:.3e}; "
+          f"vs reference program {orc.rel_l2(fast, ref):.3e}")
+    assert fast.size == oracle.size and err < 1e-4

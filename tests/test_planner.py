@@ -131,3 +131,41 @@ def test_random_geometries_against_reference_binary():
         assert p.info.ctg.n_angle == ref["ctg"]["n_angle"]
         assert p.info.ctg.add_projections == ref["ctg"]["add_projections"]
         assert _f(p.info.recon_start_pos) == _f(ref["ri"]["recon_start_pos"])
+
+
+def test_adopted_plan_runs_the_given_blocks():
+    """lct_plan_adopt keeps exactly the planner results it is given (the drop-in whole-scan
+    reconstructor adopts the reference planner's ReconData and BlockInfos this way)."""
+    import ctypes as C
+
+    from listctrecons_b200 import capi
+    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.scan import ScanGeometry
+
+    geo = ScanGeometry(ns=736, nt=64, ds=0.6, dt=0.6, npt=1152, pitch=0.8, nx=512, ny=512,
+                       dx=0.5, dz=0.5, readings=11520)
+    p = Plan(geo)
+    lib = capi.load()
+    info = capi.PlanInfo()
+    C.memmove(C.byref(info), C.byref(p.info), C.sizeof(info))
+    info.first_block, info.n_blocks_run = 3, 5
+    blocks = (capi.BlockInfo * len(p.blocks))(*p.blocks)
+    h = C.c_void_p()
+    capi.check(lib.lct_plan_adopt(C.byref(info), blocks, len(p.blocks), p.angles32.ctypes.data,
+                                  p.zpos32.ctypes.data, C.byref(h)))
+    got = capi.PlanInfo()
+    capi.check(lib.lct_plan_info_get(h, C.byref(got)))
+    assert bytes(got) == bytes(info)
+    for b in range(len(p.blocks)):
+        bi = capi.BlockInfo()
+        capi.check(lib.lct_plan_block(h, b, C.byref(bi)))
+        assert bytes(bi) == bytes(p.blocks[b])
+    lib.lct_plan_destroy(h)
+    # inconsistent inputs are refused
+    bad = capi.PlanInfo()
+    C.memmove(C.byref(bad), C.byref(info), C.sizeof(bad))
+    bad.n_blocks_run = len(p.blocks)  # first_block 3 + all blocks runs past the end
+    assert lib.lct_plan_adopt(C.byref(bad), blocks, len(p.blocks), p.angles32.ctypes.data,
+                              p.zpos32.ctypes.data, C.byref(h)) == capi.LCT_ERR_ARG
+    assert lib.lct_plan_adopt(C.byref(info), blocks, len(p.blocks) - 1, p.angles32.ctypes.data,
+                              p.zpos32.ctypes.data, C.byref(h)) == capi.LCT_ERR_ARG
