@@ -70,6 +70,11 @@ WORKLOADS = {
         geo=dict(ns=672, nt=16, ds=1.0, dt=1.0, npt=1160, pitch=1.0, nx=256, ny=256, dx=1.0, dz=1.0),
         rotations=3, blocks=1, ellipsoids=10, filter_kind=0,
         label="helical FDK 672x16@1mm, 1160 views/rot, pitch 1, >=3.7 rot, Ram-Lak, 256x256x32@1mm"),
+    "cfg5full": dict(
+        geo=dict(ns=896, nt=128, ds=0.5, dt=0.5, npt=2304, pitch=1.0, nx=1024, ny=1024, dx=0.4, dz=0.4),
+        rotations=20, blocks=0, ellipsoids=30, filter_kind=1,
+        label="helical FDK 896x128@0.5mm, 2304 views/rot, pitch 1, 20 rot as specified (every "
+              "block the planner allows), 1024x1024@0.4mm, bounded device memory"),
     "cfg5": dict(
         geo=dict(ns=896, nt=128, ds=0.5, dt=0.5, npt=2304, pitch=1.0, nx=1024, ny=1024, dx=0.4, dz=0.4),
         rotations=20, blocks=16, ellipsoids=30, filter_kind=1,
@@ -150,8 +155,10 @@ def make_workload(name: str, rank: int, world: int, blocks: int = 0):
         w["label"] = w["label"] + f" (first {blocks} blocks)"
     geo = ScanGeometry(**w["geo"])
     geo.readings = int(round(w["rotations"] * geo.npt))
-    need = w["blocks"] * world
     full = Plan(geo)
+    if not w["blocks"]:  # every block the scan allows, split over the ranks
+        w["blocks"] = full.info.n_blocks // world
+    need = w["blocks"] * world
     if full.info.n_blocks < need:  # longer scan for weak scaling / too-short configurations
         geo = geo.with_blocks(need, cap=False)
         full = Plan(geo)
@@ -800,6 +807,96 @@ def run_learned(args, rank, world, dist):
     return 0
 
 
+def run_bounded_only(args, rank, world, dist):
+    """A scan too long for whole-scan device buffers (config 5 as specified: 46,080 views,
+    21 GB of fan, 2,976 slices): only the bounded recon, host fan in (pinned) and host volume
+    out, every step; whole slabs (first and last, every acc_ystep-th row) against the FP64
+    oracle."""
+    import torch
+
+    from listctrecons_b200 import capi
+    from listctrecons_b200.recon import Reconstruction
+    from listctrecons_b200.scan import simulate_gpu
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    w, geo, plan, ph = make_workload(args.workload, rank, world, args.blocks)
+    opts = dict(mode=capi.MODE_SCAN, filter_kind=w["filter_kind"],
+                filter_mode={"fp32": capi.FILTER_FP32, "bf16x3": capi.FILTER_BF16X3, "bf16x6": capi.FILTER_BF16X6}[args.filter],
+                interp=capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT,
+                addr=capi.ADDR_BORDER, bp_nz=args.bp_nz, bp_minb=args.bp_minb)
+    rec = Reconstruction(plan, bounded=True, **opts)
+    f0, fc = rec.fan_first, rec.fan_count
+    g, ig = plan.info.ctg, plan.info.ig
+    nb = plan.info.n_blocks_run
+    log(f"[rank {rank}] bounded: views {f0}..{f0 + fc}, {nb} blocks, device "
+        f"{rec.device_bytes() / 1e9:.2f} GB")
+    h_fan = torch.empty((fc, g.nt, g.ns), dtype=torch.float32).pin_memory()
+    piece = 2048
+    for v in range(0, fc, piece):  # simulated in pieces straight into pinned host memory
+        n = min(piece, fc - v)
+        h_fan[v: v + n].copy_(simulate_gpu(geo, ph, i0=1e5, seed=7, v0=f0 + v, v1=f0 + v + n))
+    torch.cuda.synchronize()
+    h_img = torch.empty(rec.image_shape, dtype=torch.float32).pin_memory()
+    stream = torch.cuda.current_stream()
+
+    def maxr(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        rec.run(h_fan, h_img, fan_view0=f0)
+    torch.cuda.synchronize()
+    props = torch.cuda.get_device_properties(dev)
+    uuid = str(getattr(props, "uuid", "")) if hasattr(props, "uuid") else ""
+    clocks = ClockSampler(("GPU-" + uuid) if uuid and not uuid.startswith("GPU-") else (uuid or "0"))
+    time.sleep(0.3)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, _ = timed(lambda: rec.run(h_fan, h_img, fan_view0=f0), args.steps, stream)
+    ms = maxr(ms)
+    clk = clocks.stop()
+    st = rec.stats()
+    if rank != 0:
+        return 0
+    upd = st.voxel_updates * world
+    value = upd / (ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded 30-ellipsoid phantom, analytic helical scan + Poisson I0=1e5, "
+                "simulated on the GPU)",
+        "config": workload_config(w, nb, ig.ny, ig.nx, fc, g.nt, g.ns, world),
+        "options": {"mode": "scan, bounded device memory", "interp": args.interp,
+                    "filter": args.filter},
+        "s_per_volume": ms / 1e3,
+        "e2e": {"value": value, "unit": UNIT, "s_per_volume": ms / 1e3,
+                "h2d_bytes_per_step": st.h2d_bytes, "d2h_bytes_per_step": st.d2h_bytes},
+        "device_bytes": rec.device_bytes(),
+        "host_fan_bytes": fc * g.nt * g.ns * 4,
+        "volume_bytes": nb * 32 * ig.ny * ig.nx * 4,
+        "gpu_launches": st.launches * args.steps,
+        "clocks": clk,
+        "note": "every step is end to end: pinned host fan in, host volume out",
+    }
+    if not args.no_accuracy:
+        fan_dev = None
+
+        class _Fan:  # slab windows of the host fan, as the oracle check reads them
+            def __getitem__(self, sl):
+                return h_fan[sl]
+
+        line["accuracy"] = oracle_accuracy(w, plan, _Fan(), f0, h_img.numpy(), opts["interp"],
+                                           sorted({0, nb - 1}), ystep=args.acc_ystep)
+        del fan_dev
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -1057,6 +1154,8 @@ def main() -> int:
             return run_batch(args, rank, world, dist)
         if args.workload == "cfg4":
             return run_learned(args, rank, world, dist)
+        if args.workload == "cfg5full":
+            return run_bounded_only(args, rank, world, dist)
         return run_ours(args, rank, world, dist)
     finally:
         if dist is not None:

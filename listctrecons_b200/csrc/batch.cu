@@ -100,7 +100,6 @@ LCT_API int lct_batch_create(const lct_plan* const* plans, int n, const lct_reco
   // one autotune for the batch: on the scan with the most backprojection work
   const bool tune = o.bp_nz == -1;
   if (tune) o.bp_nz = 0;
-  o.bp_sampler = LCT_BP_SAMPLER_QUADS;  // the work-list kernel reads quads
   for (int i = 0; i < n && !st; ++i) {
     lct_recon* r = nullptr;
     st = lct_recon_create(plans[i], &o, &r);
@@ -119,7 +118,8 @@ LCT_API int lct_batch_create(const lct_plan* const* plans, int n, const lct_reco
       r->o.bp_minb = mb;
     }
   }
-  // work list: every scan on the quad kernel with one interpolation and thread shape
+  // work list: every scan on the quad kernel with one interpolation and thread shape (texture-
+  // sampled scans keep their own launches, as in their single-scan runs)
   if (!st) {
     b->worklist = true;
     b->interp = b->recs[0]->o.interp;
