@@ -93,6 +93,15 @@ int lct_rebin_fan2par(const lct_geom* g, const float* d_fan, float* d_par, int i
    (diagnostic; same device code as lct_rebin_fan2par). */
 int lct_rebin_fan2par_index(const lct_geom* g, int interp, int32_t* d_idx, float* d_w,
                             lct_stream stream);
+/* The scan-mode rebin (no reference counterpart as a whole-scan call; the per-view formula is
+   rebin_fan2par_kernel's, CUDA/Rebiner.cu:92-100, with the column shift alpha(is)/orbit in FP64):
+   global parallel views [g0, g0 + nviews) into d_par [nviews][nt][ns] from d_fan, whose view 0 is
+   global fan view fan_first and which holds fan_count views.  width: 0 = four columns per thread
+   (float4 rows) where the geometry allows, 1 = one column per thread, 4 = four or
+   LCT_ERR_UNSUPPORTED; every width gives the same bits. */
+int lct_rebin_fan2par_scan(const lct_geom* g, const float* d_fan, int64_t fan_first,
+                           int64_t fan_count, float* d_par, int64_t g0, int64_t nviews, int interp,
+                           int addr, int width, lct_stream stream);
 /* NullRebinerGPU::rebin + rebin_null_kernel (CUDA/Rebiner.cu:13-80) */
 int lct_rebin_null(const lct_geom* g, const float* d_fan, float* d_par, int addr,
                    lct_stream stream);

@@ -133,6 +133,7 @@ SIGNATURES: dict[str, tuple] = {
     "lct_version": (I32, []),
     "lct_rebin_fan2par": (I32, [GP, P, P, I32, I32, P]),
     "lct_rebin_fan2par_index": (I32, [GP, I32, P, P, P]),
+    "lct_rebin_fan2par_scan": (I32, [GP, P, I64, I64, P, I64, I64, I32, I32, I32, P]),
     "lct_rebin_null": (I32, [GP, P, P, I32, P]),
     "lct_rebin_pi_ori": (I32, [GP, P, P, I32, I32, P]),
     "lct_weight_pi_ori": (I32, [GP, P, P]),

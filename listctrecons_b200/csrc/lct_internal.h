@@ -124,10 +124,12 @@ int launch_bp_quad_worklist(const void* d_args, const int* d_prefix, int n_scans
 // from the fan buffer whose view 0 is global fan view `fan_first`, with the view shift of
 // column is taken from an FP64 table (alpha(is)/orbit), identical for every view.
 // fan_ring > 0: d_fan is a ring of fan_ring views (fan view v - fan_first at slot v mod ring).
+// width: 0 = four columns per thread where the geometry allows (float4 rows), 1 = one column,
+// 4 = four or LCT_ERR_UNSUPPORTED.
 int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long fan_first,
                               long long fan_count, float* d_par, long long g0,
                               long long nviews, int interp, int addr, cudaStream_t s,
-                              long long fan_ring = 0);
+                              long long fan_ring = 0, int width = 0);
 
 // BF16x3 tensor-core filter with caller-owned scratch (filter_tc.cu): tc_scratch_bytes() for
 // rows_cap rows; tc_build_toeplitz once per taps, then tc_filter per batch of rows (in place).

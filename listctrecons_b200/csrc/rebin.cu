@@ -149,6 +149,78 @@ __global__ void __launch_bounds__(256) rebin_fan2par_scan_kernel(
   }
 }
 
+// Scan mode, four consecutive columns per thread (ns a multiple of 4, so every row of four is
+// one aligned float4): a thread makes kRebinViews views x 4 columns.  The four columns' view
+// shifts floor(s) differ by at most one when 3 |ds / (dso orbit)| < 1 (the host checks), so fan
+// views f0 .. f0 + kRebinViews + 1 (f0 = the group's smallest floor) hold every tap: six float4
+// loads per row for sixteen outputs, each warp load one contiguous 512-byte row segment of one
+// fan view.  Each output is fmaf(w, t1, (1 - w) t0) with the same w, t0, t1 as the one-column
+// kernel above, so the results are bit-identical to it.
+template <int INTERP, int ADDR>
+__global__ void __launch_bounds__(256) rebin_fan2par_scan4_kernel(
+    const float* __restrict__ fan, long long fan_first, long long fan_count, long long fan_ring,
+    float* __restrict__ par, long long g0, long long nviews, RebinArgs a) {
+  constexpr int kTaps = kRebinViews + 2;
+  const long long lv = (long long)blockIdx.x * kRebinViews;
+  const int nk = (int)min((long long)kRebinViews, nviews - lv);
+  const long long g = g0 + lv;
+  const int it0 = blockIdx.y * kRebinRows;
+  const int it1 = min(a.nt, it0 + kRebinRows);
+  const long long plane = (long long)a.nt * a.ns;
+  const int groups = a.ns >> 2;
+  for (int q = threadIdx.x; q < groups; q += blockDim.x) {
+    const int is0 = q << 2;
+    float w[4];
+    long long fl[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double sc = (((double)(is0 + c) - (double)a.ws) * (double)a.ds / (double)a.dso) / (double)a.orbit;
+      const double fs = floor(sc);
+      w[c] = (float)(sc - fs);
+      if (INTERP == LCT_INTERP_TEX8) w[c] = q8(w[c]);
+      fl[c] = (long long)fs;
+    }
+    const long long f0 = min(min(fl[0], fl[1]), min(fl[2], fl[3]));
+    bool hi[4];  // the column's taps start one fan view after f0
+#pragma unroll
+    for (int c = 0; c < 4; ++c) hi[c] = fl[c] != f0;
+    const long long v0 = g + f0 - fan_first;
+    const float4* p[kTaps];
+    bool ok[kTaps];
+#pragma unroll
+    for (int m = 0; m < kTaps; ++m) {
+      long long v = v0 + m;
+      ok[m] = m <= nk + 1;
+      if (ADDR == LCT_ADDR_CLAMP)
+        v = v < 0 ? 0 : (v >= fan_count ? fan_count - 1 : v);
+      else
+        ok[m] = ok[m] && v >= 0 && v < fan_count;
+      if (!ok[m]) v = 0;
+      if (fan_ring > 0) v %= fan_ring;
+      p[m] = reinterpret_cast<const float4*>(fan + v * plane + is0);
+    }
+    float* o = par + lv * plane + is0;
+    for (int it = it0; it < it1; ++it) {
+      const long long r4 = ((long long)it * a.ns) >> 2;  // float4 offset of the row segment
+      float4 t[kTaps];
+#pragma unroll
+      for (int m = 0; m < kTaps; ++m) t[m] = ok[m] ? __ldg(p[m] + r4) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < kRebinViews; ++k) {
+        if (k < nk) {
+          const float4 lo = t[k], mid = t[k + 1], up = t[k + 2];
+          float4 out;
+          out.x = fmaf(w[0], hi[0] ? up.x : mid.x, (1.0f - w[0]) * (hi[0] ? mid.x : lo.x));
+          out.y = fmaf(w[1], hi[1] ? up.y : mid.y, (1.0f - w[1]) * (hi[1] ? mid.y : lo.y));
+          out.z = fmaf(w[2], hi[2] ? up.z : mid.z, (1.0f - w[2]) * (hi[2] ? mid.z : lo.z));
+          out.w = fmaf(w[3], hi[3] ? up.w : mid.w, (1.0f - w[3]) * (hi[3] ? mid.w : lo.w));
+          *reinterpret_cast<float4*>(o + k * plane + (long long)it * a.ns) = out;
+        }
+      }
+    }
+  }
+}
+
 // CUDA/Rebiner.cu:13-29: an offset copy (texel-centre fetch of fan view ia + add).
 template <int ADDR>
 __global__ void __launch_bounds__(256) rebin_null_kernel(const float* __restrict__ fan,
@@ -257,12 +329,30 @@ __global__ void __launch_bounds__(256) weight_pi_ori_kernel(float* __restrict__ 
 int launch_rebin_fan2par_scan(const lct_geom& g, const float* d_fan, long long fan_first,
                               long long fan_count, float* d_par, long long g0,
                               long long nviews, int interp, int addr, cudaStream_t s,
-                              long long fan_ring) {
+                              long long fan_ring, int width) {
   if (nviews <= 0) return LCT_OK;
   if (nviews > 0x7fffffffLL || fan_ring < 0) return LCT_ERR_ARG;
   RebinArgs a = rebin_args(g);
   dim3 grid((unsigned)((nviews + kRebinViews - 1) / kRebinViews), (g.nt + kRebinRows - 1) / kRebinRows);
   bool tex = interp == LCT_INTERP_TEX8, clamp = addr == LCT_ADDR_CLAMP;
+  // four columns per thread when rows are float4-aligned and a group's shifts span at most one
+  // view (3 |ds / (dso orbit)| < 1); `width` 1 forces the one-column kernel
+  const double rate = std::fabs((double)g.ds / (double)g.dso / (double)g.orbit);
+  const bool aligned = g.ns % 4 == 0 && reinterpret_cast<uintptr_t>(d_fan) % 16 == 0 &&
+                       reinterpret_cast<uintptr_t>(d_par) % 16 == 0;
+  if (width != 1 && aligned && 3.0 * rate < 1.0) {
+    const int threads = std::min(256, std::max(32, ((g.ns / 4 + 31) / 32) * 32));
+    if (tex && clamp)
+      rebin_fan2par_scan4_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, threads, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
+    else if (tex)
+      rebin_fan2par_scan4_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, threads, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
+    else if (clamp)
+      rebin_fan2par_scan4_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, threads, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
+    else
+      rebin_fan2par_scan4_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, threads, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
+    return launch_status();
+  }
+  if (width == 4) return LCT_ERR_UNSUPPORTED;
   if (tex && clamp)
     rebin_fan2par_scan_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, fan_first, fan_count, fan_ring, d_par, g0, nviews, a);
   else if (tex)
@@ -282,6 +372,18 @@ static int check_modes(int interp, int addr) {
   if (interp != LCT_INTERP_TEX8 && interp != LCT_INTERP_EXACT) return LCT_ERR_ARG;
   if (addr != LCT_ADDR_BORDER && addr != LCT_ADDR_CLAMP) return LCT_ERR_ARG;
   return LCT_OK;
+}
+
+LCT_API int lct_rebin_fan2par_scan(const lct_geom* g, const float* d_fan, int64_t fan_first,
+                                   int64_t fan_count, float* d_par, int64_t g0, int64_t nviews,
+                                   int interp, int addr, int width, lct_stream stream) {
+  int st = check_geom(g);
+  if (st) return st;
+  if ((st = check_modes(interp, addr))) return st;
+  if (!d_fan || !d_par || fan_count <= 0 || nviews < 0) return LCT_ERR_ARG;
+  if (width != 0 && width != 1 && width != 4) return LCT_ERR_ARG;
+  return launch_rebin_fan2par_scan(*g, d_fan, fan_first, fan_count, d_par, g0, nviews, interp,
+                                   addr, (cudaStream_t)stream, 0, width);
 }
 
 LCT_API int lct_rebin_fan2par(const lct_geom* g, const float* d_fan, float* d_par, int interp,

@@ -280,6 +280,20 @@ def errors(vol, target) -> dict:
             "rel_l2": float(d.norm() / target.double().norm())}
 
 
+def plain_error_percentiles(pairs, calib: float, qs=(50.0, 90.0, 99.0, 99.9)) -> dict:
+    """Percentiles of plain FDK's per-voxel error |calib * fdk - phantom|, in units of mu_water,
+    over every voxel of the first 64 pairs."""
+    torch = _torch()
+    err = torch.cat([((f.double() * calib - t.double()).abs() / MU_WATER).flatten().float()
+                     for f, t in pairs[:64]])
+    # a seeded subsample keeps torch.quantile within its input-size limit
+    if err.numel() > 8_000_000:
+        g = torch.Generator(device=err.device).manual_seed(0)
+        err = err[torch.randint(0, err.numel(), (8_000_000,), device=err.device, generator=g)]
+    qv = torch.quantile(err, torch.tensor([q / 100.0 for q in qs], device=err.device))
+    return {f"p{q:g}": float(v) for q, v in zip(qs, qv)}
+
+
 def evaluate(cnn: CNN, pairs, bound: float = DEFAULT_BOUND) -> dict:
     """Error against the phantom of plain (calibrated) FDK and of the corrected volume."""
     calib, _ = cnn.scales()
@@ -302,22 +316,26 @@ def evaluate(cnn: CNN, pairs, bound: float = DEFAULT_BOUND) -> dict:
 # ------------------------------------------------------------------------------------------
 # weights files and the training command
 # ------------------------------------------------------------------------------------------
-def save_weights(path, cnn: CNN, meta: dict) -> None:
+def save_weights(path, cnn: CNN, meta: dict, bound: float | None = None) -> None:
     import json
     from pathlib import Path
 
     calib, in_scale = cnn.scales()
     Path(path).parent.mkdir(parents=True, exist_ok=True)
+    extra = {} if bound is None else {"bound": np.float32(bound)}
     np.savez(path, params=cnn.params(), calib=np.float32(calib), in_scale=np.float32(in_scale),
-             meta=np.array(json.dumps(meta)))
+             meta=np.array(json.dumps(meta)), **extra)
 
 
 def load_weights(path) -> dict:
+    """params, calib, in_scale, meta and the acceptance-gate bound stored with the network
+    (1/mm; DEFAULT_BOUND for files that carry none)."""
     import json
 
     with np.load(path) as z:
         return {"params": z["params"].astype(np.float32), "calib": float(z["calib"]),
-                "in_scale": float(z["in_scale"]), "meta": json.loads(str(z["meta"]))}
+                "in_scale": float(z["in_scale"]), "meta": json.loads(str(z["meta"])),
+                "bound": float(z["bound"]) if "bound" in z.files else DEFAULT_BOUND}
 
 
 def cnn_from_weights(path, max_slices: int, ny: int, nx: int, train: bool = False) -> CNN:
@@ -345,9 +363,16 @@ def _train_main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--i0", type=float, default=1e5,
+                    help="photons per ray: 1e5 starves where 40 overlapping ellipsoids stack up "
+                         "(counts clamp at 1); 1e12 never clamps, so plain FDK's error is its "
+                         "cone-beam / helical artefacts and blur")
+    ap.add_argument("--gate-percentile", type=float, default=99.0,
+                    help="acceptance-gate bound stored with the network: this percentile of "
+                         "plain FDK's per-voxel error on the training pairs")
     a = ap.parse_args(argv)
     torch.cuda.set_device(0)
-    spec = pair_spec()
+    spec = pair_spec(i0=a.i0)
     gen = PairGenerator(spec, **mixed_opts())
     t0 = time.perf_counter()
     pairs = [tuple(x.clone() for x in gen.pair(100000 * (a.seed + 1) + i)) for i in range(a.pairs)]
@@ -364,17 +389,27 @@ def _train_main(argv=None) -> int:
     t_train = time.perf_counter() - t0
     inf = CNN(32, H, W, train=False)
     inf.copy_from(cnn)
+    calib = cnn.scales()[0]
+    pct = plain_error_percentiles(pairs, calib, qs=(50.0, 90.0, a.gate_percentile, 99.9))
+    bound = pct[f"p{a.gate_percentile:g}"] * MU_WATER
     meta = {
-        "geometry": "736x64@0.6mm, 1152 views/rot, pitch 1.5, 256x256x64@1mm, 40 ellipsoids, I0=1e5",
+        "geometry": f"736x64@0.6mm, 1152 views/rot, pitch 1.5, 256x256x64@1mm, 40 ellipsoids, "
+                    f"I0={a.i0:g}",
+        "i0": a.i0,
+        "plain_error_percentiles_mu_water": pct,
+        "bound_per_mm": bound,
+        "bound_rule": f"p{a.gate_percentile:g} of plain FDK's per-voxel error on the training "
+                      "pairs: the correction may move a voxel as far as plain FDK's own errors "
+                      "reach, no further",
         "recon": "scan mode, Ram-Lak, BF16x6 tensor-core filter, exact interpolation",
         "train_pairs": a.pairs, "train_seeds": f"{100000 * (a.seed + 1)}+i",
         "test_pairs": a.test_pairs, "test_seeds": f"{900000 + 1000 * a.seed}+i",
         "steps": a.steps, "batch_slices": a.batch, "lr": a.lr, "seed": a.seed,
         "pair_generation_s": t_pairs, "training_s": t_train,
-        "eval_gated": evaluate(inf, test, bound=DEFAULT_BOUND),
+        "eval_gated": evaluate(inf, test, bound=bound),
         "eval_ungated": evaluate(inf, test, bound=1e30),
     }
-    save_weights(a.out, cnn, meta)
+    save_weights(a.out, cnn, meta, bound=bound)
     print(json.dumps(meta), flush=True)
     return 0
 

@@ -70,6 +70,33 @@ def test_rebin_fan2par(setup, interp, addr):
     assert orc.rel_l2(out.cpu().numpy(), ref) < 1e-6
 
 
+@pytest.mark.parametrize("interp", [capi.INTERP_TEX8, capi.INTERP_EXACT])
+@pytest.mark.parametrize("addr", [capi.ADDR_BORDER, capi.ADDR_CLAMP])
+def test_scan_rebin_float4_columns_are_bit_identical(setup, interp, addr):
+    """The scan-mode rebin with four float4 columns per thread against one column per thread
+    (bit for bit), and against the FP64-shift oracle of the same block (1e-6): block 0's global
+    parallel views from its own fan window, including views whose taps leave the window."""
+    torch, g, fan = setup["torch"], setup["g"], setup["fan"]
+    p = setup["p"]
+    lib = capi.lib()
+    d_fan = _dev(torch, fan)
+    f0 = p.blocks[0].block_proj_start
+    g0 = f0 + g.add_projections
+    outs = []
+    for width in (1, 4):
+        out = torch.full((g.n_angle, g.nt, g.ns), float("nan"), dtype=torch.float32, device="cuda")
+        capi.check(lib.lct_rebin_fan2par_scan(C.byref(g), d_fan.data_ptr(), f0, g.n_angle_add,
+                                              out.data_ptr(), g0, g.n_angle, interp, addr, width,
+                                              None), f"width {width}")
+        _sync(torch)
+        outs.append(out.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
+    assert np.isfinite(outs[1]).all()
+    if interp == capi.INTERP_EXACT:
+        ref = orc.rebin_fan2par(g, fan, orc.EXACT, addr)
+        assert orc.rel_l2(outs[1], ref) < 1e-6
+
+
 def test_rebin_null_and_pi_ori(setup):
     torch, g, fan = setup["torch"], setup["g"], setup["fan"]
     lib = capi.lib()
