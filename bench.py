@@ -951,7 +951,8 @@ def run_ours(args, rank, world, dist):
                 interp=capi.INTERP_TEX8 if args.interp == "tex8" else capi.INTERP_EXACT,
                 addr=capi.ADDR_BORDER, bp_nz=args.bp_nz, bp_minb=args.bp_minb,
                 bp_sampler={"auto": capi.BP_SAMPLER_AUTO, "quads": capi.BP_SAMPLER_QUADS,
-                            "texture": capi.BP_SAMPLER_TEXTURE}[args.sampler])
+                            "texture": capi.BP_SAMPLER_TEXTURE,
+                            "tma": capi.BP_SAMPLER_QUADS_TMA}[args.sampler])
     rec = Reconstruction(plan, **opts)
     tuned = rec.autotune() if args.bp_nz == -1 else None  # the choice cached at create
     st = rec.stats()
@@ -1074,7 +1075,8 @@ def run_ours(args, rank, world, dist):
     own_gbs = upd * 16 / (bp / 1e3) / 1e9
     hbm_gbs = hbm_bytes / (bp / 1e3) / 1e9
     texture = args.interp == "tex8" and args.sampler in ("auto", "texture")
-    kernel = "bp_tex_kernel" if texture else "bp_quad_kernel"
+    tma = args.interp == "exact" and args.sampler == "tma"
+    kernel = "bp_tex_kernel" if texture else ("bp_tma_kernel" if tma else "bp_quad_kernel")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -1083,7 +1085,7 @@ def run_ours(args, rank, world, dist):
         "data": "synthetic (seeded 30-ellipsoid phantom, analytic helical scan + Poisson I0=1e5, simulated on the GPU)",
         "config": workload_config(w, nb, ig.ny, ig.nx, fc, g.nt, g.ns, world),
         "options": {"mode": args.mode, "interp": args.interp, "filter": args.filter,
-                    "sampler": "texture" if texture else "quads",
+                    "sampler": "texture" if texture else ("quads, TMA-staged" if tma else "quads"),
                     "bp_nz": tuned[0] if tuned else (args.bp_nz or "auto"),
                     "bp_minb": tuned[1] if tuned else (args.bp_minb or "auto"),
                     "bp_tuning": "autotuned at create" if tuned else "fixed",
@@ -1152,9 +1154,10 @@ def main() -> int:
     ap.add_argument("--bp-nz", type=int, default=0,
                     help="slices per backprojection thread: 4, 8, 16; 0 = default; -1 = autotune")
     ap.add_argument("--bp-minb", type=int, default=0)
-    ap.add_argument("--sampler", default="auto", choices=["auto", "quads", "texture"],
-                    help="backprojection sampler: quads (16-byte 2x2 texel loads) or the texture "
-                         "unit (TEX8 only); auto = texture for tex8, quads for exact")
+    ap.add_argument("--sampler", default="auto", choices=["auto", "quads", "texture", "tma"],
+                    help="backprojection sampler: quads (16-byte 2x2 texel loads through L1), "
+                         "the texture unit (TEX8 only), or quads staged in shared memory by TMA "
+                         "(exact only); auto = texture for tex8, quads for exact")
     ap.add_argument("--blocks", type=int, default=0, help="override the blocks per GPU (profiling)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
     ap.add_argument("--ref-budget", type=float, default=4.0,

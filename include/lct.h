@@ -255,10 +255,13 @@ void lct_plan_destroy(lct_plan* plan);
             interpolation);
    TEXTURE  views in a 3-D texture, one hardware fetch per sample (TEX8 only: the reference's own
             fetch, CUDA/Backprojector.cu:85-86; falls back to QUADS otherwise);
+   QUADS_TMA (EXACT only) the quads, with each view's tile footprint staged in shared memory by
+            TMA before the samples read it (the same values: bit-identical to QUADS);
    AUTO     TEXTURE for TEX8, QUADS for EXACT. */
 #define LCT_BP_SAMPLER_AUTO 0
 #define LCT_BP_SAMPLER_QUADS 1
 #define LCT_BP_SAMPLER_TEXTURE 2
+#define LCT_BP_SAMPLER_QUADS_TMA 3
 
 typedef struct lct_recon_opts {
   int mode;          /* LCT_MODE_* */

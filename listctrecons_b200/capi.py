@@ -30,7 +30,7 @@ MODE_BLOCK, MODE_SCAN = 0, 1
 REBIN_FAN2PAR, REBIN_NULL, REBIN_PI_ORI = 0, 1, 2
 PW_NONE, PW_PI_ORI = 0, 1
 BP_PAR, BP_PI_ORI = 0, 1
-BP_SAMPLER_AUTO, BP_SAMPLER_QUADS, BP_SAMPLER_TEXTURE = 0, 1, 2
+BP_SAMPLER_AUTO, BP_SAMPLER_QUADS, BP_SAMPLER_TEXTURE, BP_SAMPLER_QUADS_TMA = 0, 1, 2, 3
 
 
 class LctError(RuntimeError):

@@ -20,9 +20,11 @@
 // footprint; a polynomial asin on tiles within dso / 2 of the axis.
 #include <climits>
 #include <cmath>
+#include <mutex>
 #include <type_traits>
 
 #include "lct_internal.h"
+#include "tc_ptx.cuh"
 #include "tex_emul.cuh"
 
 namespace lct {
@@ -493,6 +495,287 @@ __global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_
   bp_quad_tile<NZ, INTERP, PART>(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// EXACT with every view's tile footprint staged in shared memory by TMA.  Per view pair the
+// footprint boxes of the view and of its conjugate -- kTmaBH quad rows x kTmaBW quad columns each,
+// from the tile's corners at its first and last slice (the prefetch boxes above) -- are loaded
+// with one cp.async.bulk.tensor each (no multicast) into a kTmaStages-deep ring, one mbarrier per
+// stage for "landed" (transaction bytes) and one for "consumed" (one arrive per warp).  Thread 0
+// issues the loads kTmaStages views ahead.  The samples then read shared memory: the same
+// floor / fraction / bit-pattern arithmetic as the global path, the address one 32-bit multiply-add
+// into the box.  Every warp checks, per view, that its lanes' quad rows (first and last slice:
+// rows are monotone in the slice) and columns lie inside the boxes; a warp that is not inside,
+// or a view whose footprint exceeds a box, reads global memory as the quad kernel does, so the
+// result never depends on the box estimate.  Bit-identical to bp_quad_kernel (same arithmetic
+// on the same quad values).  Every mbarrier wait is bounded.
+constexpr int kTmaBW = 36;   // quad columns per box
+constexpr int kTmaBH = 16;   // quad rows per box
+constexpr int kTmaStages = 2;
+constexpr unsigned kTmaRowBytes = kTmaBW * 16;
+constexpr unsigned kTmaBoxBytes = kTmaBW * kTmaBH * 16;
+constexpr unsigned kTmaStageBytes = 2 * kTmaBoxBytes;
+constexpr int kTmaSmem = kTmaStages * kTmaStageBytes + 128;  // + alignment slack
+
+template <int NZ>
+__device__ __forceinline__ void bp_tma_tile(const BpQuadArgs& A, const CUtensorMap* map, int bx,
+                                            int by, int bz, uint32_t stage0, uint32_t full0,
+                                            uint32_t empty0, int* status) {
+  __shared__ float4 s_cs[kQVB];       // cos, sin of view ia and of its conjugate ia + half
+  __shared__ int2 s_jr[kQVB];         // slices [jlo, jhi) of the chunk whose window holds ia
+  __shared__ float2 s_zb[kQVB];       // source z of both views without the fan-angle term
+  __shared__ ulonglong2 s_qv[kQVB];   // biased global bases of both views (the fallback)
+  __shared__ int4 s_box[kQVB];        // box origins: row0, col0 of the view and of the conjugate
+  __shared__ int2 s_slot[kQVB];       // quad-buffer view slots (TMA z) of both views; x < 0: no box
+  __shared__ int s_abort;
+
+  const int tid = threadIdx.y * kQTX + threadIdx.x;
+  const int lane = tid & 31;
+  const int ix = bx * kQTX + threadIdx.x;
+  const int iy = by * kQTY + threadIdx.y;
+  const int slab = bz / A.zchunks;
+  const int z0 = (bz % A.zchunks) * NZ;
+  const int nzc = min(NZ, A.nz - z0);
+
+  const float xc = __fmul_rn((float)ix - A.wx, A.dx);
+  const float yc = __fmul_rn((float)iy - A.wy, A.dy);
+  const float zc0 = __fmul_rn((float)z0 - A.wz, A.dz);
+  const float wt2 = A.wt + 2.0f;
+  const float xr0 = __fmul_rn((float)(bx * kQTX) - A.wx, A.dx);
+  const float xr1 = __fmul_rn((float)(min(bx * kQTX + kQTX, A.nx) - 1) - A.wx, A.dx);
+  const float yr0 = __fmul_rn((float)(by * kQTY) - A.wy, A.dy);
+  const float yr1 = __fmul_rn((float)(min(by * kQTY + kQTY, A.ny) - 1) - A.wy, A.dy);
+  const float zcl = __fmul_rn((float)(z0 + nzc - 1) - A.wz, A.dz);
+  const float rx = fmaxf(fabsf(xr0), fabsf(xr1)), ry = fmaxf(fabsf(yr0), fabsf(yr1));
+  const bool asin_poly = sqrtf(fmaf(rx, rx, ry * ry)) * A.inv_dso < 0.49f;
+
+  int vlo = INT_MAX, vhi = INT_MIN;
+  for (int j = 0; j < nzc; ++j) {
+    vlo = min(vlo, A.a_min[z0 + j]);
+    vhi = max(vhi, A.a_mid[z0 + j]);
+  }
+  const int sv = A.slab_view[slab];
+  const float* betas = A.betas + sv;
+  const float wt = A.wt;
+  float acc[NZ];
+#pragma unroll
+  for (int j = 0; j < NZ; ++j) acc[j] = 0.0f;
+  if (tid == 0) s_abort = 0;
+  long long kk = 0;  // ring uses so far (stage = kk mod kTmaStages, phase = kk / kTmaStages)
+
+  // thread 0: the loads of batch view q (ring use kq) into its stage; a plain arrive when the
+  // view has no box, so the stage's "landed" phase completes either way
+  auto issue = [&](int q, long long kq) {
+    const int st = (int)(kq % kTmaStages);
+    const uint32_t fb = full0 + 8 * st;
+    const int2 sl = s_slot[q];
+    if (sl.x < 0 || s_abort) {
+      mbar_arrive(fb);
+      return;
+    }
+    const int4 b = s_box[q];
+    mbar_expect_tx(fb, kTmaStageBytes);
+    const uint32_t dst = stage0 + st * kTmaStageBytes;
+    tma_load_3d(dst, map, 4 * b.y, b.x, sl.x, fb);
+    tma_load_3d(dst + kTmaBoxBytes, map, 4 * b.w, b.z, sl.y, fb);
+  };
+
+  for (int vb = vlo; vb < vhi; vb += kQVB) {
+    __syncthreads();
+    if (tid < kQVB && vb + tid < vhi) {
+      const int ia = vb + tid;
+      float c1, s1, c2, s2;
+      view_trig_pi(betas, ia, c1, s1);
+      view_trig_pi(betas, ia + A.half, c2, s2);
+      s_cs[tid] = make_float4(c1, s1, c2, s2);
+      const float4* v1 = quad_view_ptr(A, sv, ia);
+      const float4* v2 = quad_view_ptr(A, sv, ia + A.half);
+      s_zb[tid] = make_float2(fmaf((float)ia, A.dzv, A.z0), fmaf((float)(ia + A.half), A.dzv, A.z0));
+      s_qv[tid] = make_ulonglong2(quad_view_bias(v1, A.qrow_bytes), quad_view_bias(v2, A.qrow_bytes));
+      int4 b1, b2;
+      prefetch_boxes(A, c1, s1, c2, s2, ia, xr0, xr1, yr0, yr1, zc0, zcl, b1, b2);
+      const bool fits = b1.y - b1.x + 1 <= kTmaBH && b1.w - b1.z + 1 <= kTmaBW &&
+                        b2.y - b2.x + 1 <= kTmaBH && b2.w - b2.z + 1 <= kTmaBW;
+      s_box[tid] = make_int4(b1.x, b1.z, b2.x, b2.z);
+      const long long q1 = (long long)(v1 - A.quads) / A.qstride;
+      const long long q2 = (long long)(v2 - A.quads) / A.qstride;
+      s_slot[tid] = fits ? make_int2((int)q1, (int)q2) : make_int2(-1, -1);
+      int jlo = nzc, jhi = 0;
+      for (int j = 0; j < nzc; ++j)
+        if (ia >= A.a_min[z0 + j] && ia < A.a_mid[z0 + j]) {
+          jlo = min(jlo, j);
+          jhi = max(jhi, j + 1);
+        }
+      s_jr[tid] = make_int2(jlo, jhi);
+    }
+    __syncthreads();
+    const int nv = min(kQVB, vhi - vb);
+    const long long kbase = kk;
+    if (tid == 0)
+      for (int q = 0; q < kTmaStages && q < nv; ++q) issue(q, kbase + q);
+    for (int k = 0; k < nv; ++k) {
+      const long long kq = kbase + k;
+      const int st = (int)(kq % kTmaStages);
+      const uint32_t parity = (uint32_t)((kq / kTmaStages) & 1);
+      const int2 sl = s_slot[k];
+      bool smem_ok = sl.x >= 0;
+      if (!mbar_wait(full0 + 8 * st, parity)) {  // bounded: a load that never lands
+        if (status) atomicExch(status, kDevWaitTimeout);
+        s_abort = 1;
+        smem_ok = false;
+      }
+      const int2 jr = s_jr[k];
+      const int jlo = jr.x, jhi = jr.y;
+      const float4 cs = s_cs[k];
+      const float cb = cs.x, sb = cs.y, cb2 = cs.z, sb2 = cs.w;
+      const float phat = fmaf(-xc, cb, -__fmul_rn(yc, sb));
+      const float sx = __fmul_rn(phat, A.inv_dso);
+      const float theta = asin_poly ? asin_half(sx) : asinf(sx);
+      const float tho = __fmul_rn(theta, A.inv_orbit);
+      const float tq = fmaf(-phat, phat, A.dso2);
+      const float sq = __fmul_rn(tq, rsqrtf(tq));
+      const float l1 = fmaf(xc, sb, fmaf(-yc, cb, sq));
+      const float l2 = fmaf(xc, sb2, fmaf(-yc, cb2, sq));
+      const float2 zb = s_zb[k];
+      const ulonglong2 qv = s_qv[k];
+      const float zr1 = fmaf(tho, A.dzv, zb.x), zr2 = fmaf(-tho, A.dzv, zb.y);
+      const float r1 = __fdividef(1.0f, l1), r2 = __fdividef(1.0f, l2);
+      const float kd1 = __fmul_rn(A.kqdz, r1), kd2 = __fmul_rn(A.kqdz, r2);
+      const float h1 = __fmul_rn(__fsub_rn(zc0, zr1), __fmul_rn(A.kq, r1));
+      const float h2 = __fmul_rn(__fsub_rn(zc0, zr2), __fmul_rn(A.kq, r2));
+      const float u1 = __fadd_rn(h1, wt2), u2 = __fadd_rn(h2, wt2);
+      float a1, a2;
+      const unsigned long long q1 = quad_col_exact(qv.x, fmaf(theta, A.dso_over_ds, A.ws), A.ns, a1);
+      const unsigned long long q2 = quad_col_exact(qv.y, fmaf(-theta, A.dso_over_ds, A.ws), A.ns, a2);
+      // the thread's quad columns (0 .. ns + 2) and its first / last slice's quad rows
+      const int qc1 = (int)((q1 - qv.x) >> 4) - (kMagicBits - 2);
+      const int qc2 = (int)((q2 - qv.y) >> 4) - (kMagicBits - 2);
+      auto qrow = [&](float u) {
+        const int rb = __float_as_int(__fadd_rd(u, kMagic));
+        return min(max(rb, kMagicBits), kMagicBits + A.nt + 2) - kMagicBits;
+      };
+      const int4 bo = s_box[k];
+      bool in_box = false;
+      if (smem_ok && jlo < jhi) {
+        const float fa = (float)jlo, fb = (float)(jhi - 1);
+        const int ra1 = qrow(fmaf(fa, kd1, u1)), rb1 = qrow(fmaf(fb, kd1, u1));
+        const int ra2 = qrow(fmaf(fa, kd2, u2)), rb2 = qrow(fmaf(fb, kd2, u2));
+        in_box = min(ra1, rb1) >= bo.x && max(ra1, rb1) < bo.x + kTmaBH && qc1 >= bo.y &&
+                 qc1 < bo.y + kTmaBW && min(ra2, rb2) >= bo.z && max(ra2, rb2) < bo.z + kTmaBH &&
+                 qc2 >= bo.w && qc2 < bo.w + kTmaBW;
+      } else if (smem_ok) {
+        in_box = true;  // no slice of this thread uses the view
+      }
+      const bool use_smem = __all_sync(0xffffffffu, in_box);
+      // shared-memory bases biased like the global ones: + row bit pattern * row bytes
+      const uint32_t sbase = stage0 + st * kTmaStageBytes;
+      const uint32_t sbv = sbase + 16u * (uint32_t)(qc1 - bo.y) -
+                           (uint32_t)(kMagicBits + bo.x) * kTmaRowBytes;
+      const uint32_t sbc = sbase + kTmaBoxBytes + 16u * (uint32_t)(qc2 - bo.w) -
+                           (uint32_t)(kMagicBits + bo.z) * kTmaRowBytes;
+      auto sample = [&](bool smem, bool clamp, unsigned long long gq, uint32_t sq0, float a,
+                        float u) -> float {
+        const float t = __fadd_rd(u, kMagic);
+        const float b = u - (t - kMagic);
+        int rb = __float_as_int(t);
+        if (clamp) rb = min(max(rb, kMagicBits), kMagicBits + A.nt + 2);
+        const float4 v = smem ? lds128(sq0 + (uint32_t)rb * kTmaRowBytes)
+                              : __ldg(reinterpret_cast<const float4*>(
+                                    gq + (unsigned long long)(unsigned)rb * A.qrow_bytes));
+        return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
+      };
+      auto slice_x = [&](int j, auto inside, auto smem) {
+        const float fj = (float)j;
+        const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
+        const float in1 = -qh2 * __fdividef(1.0f, qh1 - qh2);
+        float w1 = in1;
+        if constexpr (!decltype(inside)::value) {
+          const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
+          w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
+        }
+        constexpr bool kClamp = !decltype(inside)::value;
+        constexpr bool kSmem = decltype(smem)::value;
+        const float s1 = sample(kSmem, kClamp, q1, sbv, a1, fmaf(fj, kd1, u1));
+        const float s2 = sample(kSmem, kClamp, q2, sbc, a2, fmaf(fj, kd2, u2));
+        acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
+      };
+      bool inside = false;
+      if (jlo == 0 && jhi == NZ) {
+        const float e1 = fmaf((float)(NZ - 1), kd1, h1), e2 = fmaf((float)(NZ - 1), kd2, h2);
+        inside = A.rows_inside_ok && fabsf(h1) <= wt && fabsf(e1) <= wt && fabsf(h2) <= wt &&
+                 fabsf(e2) <= wt;
+      }
+      const bool all_inside = __all_sync(0xffffffffu, inside);
+      if (use_smem) {
+        if (all_inside) {
+#pragma unroll
+          for (int j = 0; j < NZ; ++j) slice_x(j, std::true_type{}, std::true_type{});
+        } else {
+#pragma unroll
+          for (int j = 0; j < NZ; ++j)
+            if (j >= jlo && j < jhi) slice_x(j, std::false_type{}, std::true_type{});
+        }
+      } else {
+        if (all_inside) {
+#pragma unroll
+          for (int j = 0; j < NZ; ++j) slice_x(j, std::true_type{}, std::false_type{});
+        } else {
+#pragma unroll
+          for (int j = 0; j < NZ; ++j)
+            if (j >= jlo && j < jhi) slice_x(j, std::false_type{}, std::false_type{});
+        }
+      }
+      // this warp is done with the stage; thread 0 refills it kTmaStages views ahead
+      __syncwarp();
+      if (lane == 0) mbar_arrive(empty0 + 8 * st);
+      if (tid == 0 && k + kTmaStages < nv) {
+        if (!mbar_wait(empty0 + 8 * st, parity)) {
+          if (status) atomicExch(status, kDevWaitTimeout);
+          s_abort = 1;
+        }
+        issue(k + kTmaStages, kq + kTmaStages);
+      }
+    }
+    kk = kbase + nv;
+  }
+  // after a wait that ran out, the copies still in flight land before the CTA exits (bounded)
+  if (tid == 0 && s_abort)
+    for (long long kq = (kk > kTmaStages ? kk - kTmaStages : 0); kq < kk; ++kq)
+      mbar_wait(full0 + 8 * (int)(kq % kTmaStages), (uint32_t)((kq / kTmaStages) & 1));
+  __syncthreads();
+
+  if (ix < A.nx && iy < A.ny) {
+    float* out = A.img + ((long long)(A.slab_z0[slab] + z0) * A.ny + iy) * A.nx + ix;
+    const long long plane = (long long)A.nx * A.ny;
+#pragma unroll
+    for (int j = 0; j < NZ; ++j) {
+      if (j < nzc) {
+        const int span = A.a_max[z0 + j] - A.a_min[z0 + j];
+        // CUDA/Backprojector.cu:96 in double; x4 restores the halved weights and the pair doubling
+        out[j * plane] = span > 0 ? (float)((double)(acc[j] * 4.0f) * kRefPi / (double)(float)span) : 0.0f;
+      }
+    }
+  }
+}
+
+template <int NZ, int MINB>
+__global__ void __launch_bounds__(kQTX* kQTY, MINB)
+    bp_tma_kernel(const __grid_constant__ BpQuadArgs A, const __grid_constant__ CUtensorMap map,
+                  int* status) {
+  extern __shared__ uint8_t tma_smem_raw[];
+  __shared__ __align__(8) uint64_t bars[2 * kTmaStages];
+  const uint32_t stage0 = (smem_u32(tma_smem_raw) + 127u) & ~127u;
+  const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[kTmaStages]);
+  const int tid = threadIdx.y * kQTX + threadIdx.x;
+  if (tid == 0) {
+    for (int s = 0; s < kTmaStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, kQTX * kQTY / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  bp_tma_tile<NZ>(A, &map, blockIdx.x, blockIdx.y, blockIdx.z, stage0, full0, empty0, status);
+}
+
 // TEX8 sampled by the texture unit itself: the filtered views in a 3-D cudaArray (x = column,
 // y = row, z = view slot; cudaFilterModeLinear, unnormalised, the recon's addressing) and every
 // sample one tex3D at (p_idx + 0.5, q_idx + 0.5, slot + 0.5) -- the reference's own fetch
@@ -775,6 +1058,48 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
   }
 #undef LCT_BPQ_NZ
 #undef LCT_BPQ
+  return launch_status();
+}
+
+// Tensor map of a quad buffer for the TMA-staged kernel: 3-D float tensor {4 (ns + 3) floats,
+// nt + 3 rows, views}, box {4 kTmaBW, kTmaBH, 1}, no swizzle, out-of-range reads as zero.
+int bp_tma_map(CUtensorMap* map, const float4* quads, int ns, int nt, long long views) {
+  auto fn = tensor_map_encoder();
+  if (!fn) return LCT_ERR_UNSUPPORTED;
+  if (reinterpret_cast<uintptr_t>(quads) % 16 != 0 || views <= 0 || views > 0x7fffffffLL)
+    return LCT_ERR_ARG;
+  const cuuint64_t dims[3] = {(cuuint64_t)(4 * quad_cols(ns)), (cuuint64_t)(nt + 3),
+                              (cuuint64_t)views};
+  const cuuint64_t strides[2] = {(cuuint64_t)(16 * quad_cols(ns)),
+                                 (cuuint64_t)(16 * quad_view_elems(ns, nt))};
+  const cuuint32_t box[3] = {(cuuint32_t)(4 * kTmaBW), (cuuint32_t)kTmaBH, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float4*>(quads), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? LCT_OK : LCT_ERR_UNSUPPORTED;
+}
+
+int launch_bp_par_quads_tma(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                            const float4* quads, const CUtensorMap& map, cudaStream_t s) {
+  if (L.interp != LCT_INTERP_EXACT) return LCT_ERR_UNSUPPORTED;
+  const bool part = L.part != kBpWhole || L.view_lo > 0 || L.view_hi < (1 << 30);
+  if (part) return launch_bp_par_quads(g, ig, L, quads, s);  // parts stay on the L1 kernel
+  static thread_local BpQuadArgs a;
+  int nzt = 8;
+  int st = build_bp_quad_args(g, ig, L, quads, a, nzt);
+  if (st) return st;
+  if (nzt != 8) return launch_bp_par_quads(g, ig, L, quads, s);  // the staged kernel is NZ 8
+  dim3 grid(a.gx, a.gy, a.gz);
+  dim3 block(kQTX, kQTY);
+  int minb = L.minb;
+  if (minb < 2 || minb > 4) minb = 4;
+  int* status = device_status_ptr();
+  switch (minb) {
+    case 2: bp_tma_kernel<8, 2><<<grid, block, kTmaSmem, s>>>(a, map, status); break;
+    case 3: bp_tma_kernel<8, 3><<<grid, block, kTmaSmem, s>>>(a, map, status); break;
+    default: bp_tma_kernel<8, 4><<<grid, block, kTmaSmem, s>>>(a, map, status);
+  }
   return launch_status();
 }
 

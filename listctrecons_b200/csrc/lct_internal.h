@@ -1,6 +1,7 @@
 // Internal helpers shared by the liblct translation units (not installed, not part of the ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -92,6 +93,12 @@ int launch_quad_pack(const float* rows, long long views, int ns, int nt, int add
 // Backprojection from quad-layout views (full windows only; L.proj is ignored, L.quads used).
 int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
                         const float4* quads, cudaStream_t s);
+// EXACT backprojection with each view's tile footprint staged in shared memory by TMA (the
+// quads' tensor map from bp_tma_map, over the same quad buffer); whole launches with 8 slices per
+// thread (other launches go to launch_bp_par_quads).
+int bp_tma_map(CUtensorMap* map, const float4* quads, int ns, int nt, long long views);
+int launch_bp_par_quads_tma(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
+                            const float4* quads, const CUtensorMap& map, cudaStream_t s);
 // Backprojection sampled by the texture unit (TEX8 only): tex holds the filtered views as a
 // 3-D array, slab s's local view ia at z slot (slab_view[s] + ia) mod L.quad_ring (0: no wrap).
 int launch_bp_par_texture(const lct_geom& g, const lct_img& ig, const BpLaunch& L,

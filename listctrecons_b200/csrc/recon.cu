@@ -137,6 +137,8 @@ int recon_setup(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** ou
   }
   r->quads = o.backprojector == LCT_BP_PAR && bp_windows_full(g, r->info.ig, kBlockSlices);
   r->tex_bp = want_texture(o, r->quads);
+  r->tma_bp = r->quads && !r->tex_bp && o.interp == LCT_INTERP_EXACT &&
+              o.bp_sampler == LCT_BP_SAMPLER_QUADS_TMA;
   *out = r;
   return LCT_OK;
 }
@@ -210,6 +212,8 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
     if (r->quads && !r->tex_bp &&
         (st = alloc((void**)&r->d_quad, sizeof(float4) * par_views * quad_view_elems(g.ns, g.nt))))
       break;
+    if (r->tma_bp && bp_tma_map(&r->tma_map, r->d_quad, g.ns, g.nt, par_views) != LCT_OK)
+      r->tma_bp = false;  // no tensor-map encoder in this driver: the L1 quad kernel
     if (o.filter_mode != LCT_FILTER_FP32) r->tc_rows = par_views * g.nt;
     st = recon_alloc_common(r, plan);
   } while (0);
@@ -246,7 +250,8 @@ LCT_API int lct_recon_autotune(lct_recon* r, int* nz_out, int* minb_out) {
   static std::map<std::vector<long long>, std::pair<int, int>> cache;
   const std::vector<long long> key = {g.ns, g.nt, ig.nx, ig.ny, g.n_angle, g.n_proj_turn,
                                       r->o.interp, (long long)(1000.0 * g.pitch / ig.dz),
-                                      (long long)r->info.n_blocks_run, (long long)r->tex_bp};
+                                      (long long)r->info.n_blocks_run, (long long)r->tex_bp,
+                                      (long long)r->tma_bp};
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
@@ -470,6 +475,7 @@ int recon_pack(lct_recon* r, const float* par, long long nv, long long v0, int a
 int recon_bp_pairs(lct_recon* r, BpLaunch& L, cudaStream_t s) {
   L.quad_ring = r->quad_ring;
   if (r->tex_bp) return launch_bp_par_texture(r->info.ctg, r->info.ig, L, r->vtex.tex, s);
+  if (r->tma_bp) return launch_bp_par_quads_tma(r->info.ctg, r->info.ig, L, r->d_quad, r->tma_map, s);
   return launch_bp_par_quads(r->info.ctg, r->info.ig, L, r->d_quad, s);
 }
 

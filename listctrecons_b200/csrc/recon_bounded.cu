@@ -605,6 +605,8 @@ LCT_API int lct_recon_create_bounded(const lct_plan* plan, const lct_recon_opts*
     if (!r->tex_bp &&
         (st = alloc((void**)&r->d_quad, sizeof(float4) * quad_views * quad_view_elems(g.ns, g.nt))))
       break;
+    if (r->tma_bp && bp_tma_map(&r->tma_map, r->d_quad, g.ns, g.nt, quad_views) != LCT_OK)
+      r->tma_bp = false;
     if (r->o.filter_mode != LCT_FILTER_FP32) r->tc_rows = P * g.nt;
     st = recon_alloc_common(r, plan);
   } while (0);
