@@ -1074,7 +1074,7 @@ def run_ours(args, rank, world, dist):
     alg_gbs = upd * 32 / (bp / 1e3) / 1e9
     own_gbs = upd * 16 / (bp / 1e3) / 1e9
     hbm_gbs = hbm_bytes / (bp / 1e3) / 1e9
-    texture = args.interp == "tex8" and args.sampler in ("auto", "texture")
+    texture = args.interp == "tex8" and args.sampler == "texture"
     tma = args.interp == "exact" and args.sampler == "tma"
     kernel = "bp_tex_kernel" if texture else ("bp_tma_kernel" if tma else "bp_quad_kernel")
 
@@ -1157,7 +1157,7 @@ def main() -> int:
     ap.add_argument("--sampler", default="auto", choices=["auto", "quads", "texture", "tma"],
                     help="backprojection sampler: quads (16-byte 2x2 texel loads through L1), "
                          "the texture unit (TEX8 only), or quads staged in shared memory by TMA "
-                         "(exact only); auto = texture for tex8, quads for exact")
+                         "(exact only); auto = quads")
     ap.add_argument("--blocks", type=int, default=0, help="override the blocks per GPU (profiling)")
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU work per sample")
     ap.add_argument("--ref-budget", type=float, default=4.0,

@@ -348,57 +348,105 @@ __global__ void __launch_bounds__(kBpTX* kBpTY) bp_par_general_kernel(const __gr
   }
 }
 
-// ---------------------------------------------------------------------------------------
-// PI-window backprojection (CUDA/Backprojector.cu:171-250), one thread per voxel.
-// ---------------------------------------------------------------------------------------
+// PI-window backprojection with NZ slices per thread: the view terms that do not depend on the
+// slice (cos/sin, s, gamma, temp1, the in-plane distance, the column setup) are evaluated once per
+// (voxel column, view) and shared by every slice whose walk visits the view; each slice keeps its
+// own a_middle, its own stop of the backward walk (|t| > pitch / 4) and its own forward range, and
+// sums its views in the reference's order (backward from a_middle, then forward from
+// a_middle + 1), with the reference's expression for t (CUDA/Backprojector.cu:200-245).
+constexpr int kPiNZ = 8;
 template <int INTERP, int ADDR>
-__global__ void __launch_bounds__(256) bp_pi_ori_kernel(const __grid_constant__ BpArgsDev A) {
+__global__ void __launch_bounds__(256) bp_pi_ori_z_kernel(const __grid_constant__ BpArgsDev A) {
   const int ix = blockIdx.x * kBpTX + threadIdx.x;
   const int iy = blockIdx.y * kBpTY + threadIdx.y;
-  const int iz = blockIdx.z;
+  const int z0 = blockIdx.z * kPiNZ;
   if (ix >= A.nx || iy >= A.ny) return;
+  const int nzc = min(kPiNZ, A.nz - z0);
   const float xc = ((float)ix - A.wx) * A.dx;
   const float yc = ((float)iy - A.wy) * A.dy;
-  const float zc = ((float)iz - A.wz) * A.dz;
-  int a_middle = (int)roundf((zc - A.z0) / A.dzv);
-  a_middle = a_middle < 0 ? 0 : a_middle;
-  a_middle = a_middle > A.n_angle - 1 ? A.n_angle - 1 : a_middle;
   const float pitch = A.pitch;
   const float t2 = (float)((double)pitch / (2 * kRefPi));  // :209, double through PI
-  float sum = 0.0f;
-  int ia;
-  auto contrib = [&](int v, bool& stop, bool check) -> float {
+  float zc[kPiNZ], sum[kPiNZ];
+  int amid[kPiNZ], amin[kPiNZ];
+  unsigned walking = 0;  // bit j: slice j's backward walk has not stopped
+  int vtop = -1;
+#pragma unroll
+  for (int j = 0; j < kPiNZ; ++j) {
+    zc[j] = ((float)(z0 + j) - A.wz) * A.dz;
+    int a = (int)roundf((zc[j] - A.z0) / A.dzv);
+    a = a < 0 ? 0 : a;
+    a = a > A.n_angle - 1 ? A.n_angle - 1 : a;
+    amid[j] = a;
+    amin[j] = -1;
+    sum[j] = 0.0f;
+    if (j < nzc) {
+      walking |= 1u << j;
+      vtop = max(vtop, a);
+    }
+  }
+  // the slice-invariant terms of view v
+  struct ViewTerms {
+    float temp1, gt2, den;
+    ColSetup c;
+    const float* view;
+  };
+  auto terms = [&](int v) {
+    ViewTerms w;
     float cb, sb;
     view_trig(A.betas, v, cb, sb);
     const float s = -xc * cb - yc * sb;
     const float gamma = asinf(s / A.dso);
-    const float temp1 = sqrtf(A.dso * A.dso - s * s);
-    const float zoff = zc - (A.z0 + A.dzv * (float)v);
-    float t = temp1 * (zoff - gamma * t2) / (temp1 + xc * sb - yc * cb) + gamma * t2;
-    t *= A.zdir;
-    if (check && (t > pitch / 4 || t < -pitch / 4)) {
-      stop = true;
-      return 0.0f;
-    }
-    const float is = s / A.ds + A.ws;
-    const float it = t * 2 * (A.nt - 1) / pitch + A.wt;
-    const ColSetup c = col_setup<INTERP, ADDR>(is, A.ns);
-    return sample_rows<INTERP, ADDR>(A.proj + (long long)v * A.view_stride, A.ns, A.nt, c, it);
+    w.temp1 = sqrtf(A.dso * A.dso - s * s);
+    w.gt2 = gamma * t2;
+    w.den = w.temp1 + xc * sb - yc * cb;
+    w.c = col_setup<INTERP, ADDR>(s / A.ds + A.ws, A.ns);
+    w.view = A.proj + (long long)v * A.view_stride;
+    return w;
   };
-  for (ia = a_middle; ia >= 0; --ia) {
-    bool stop = false;
-    float c = contrib(ia, stop, true);
-    if (stop) break;
-    sum += c;
+  auto tval = [&](const ViewTerms& w, float zcj, int v) {
+    const float zoff = zcj - (A.z0 + A.dzv * (float)v);
+    float t = w.temp1 * (zoff - w.gt2) / w.den + w.gt2;
+    return t * A.zdir;
+  };
+  // backward walks, views descending; slice j joins at its a_middle
+  for (int v = vtop; v >= 0 && walking; --v) {
+    const ViewTerms w = terms(v);
+#pragma unroll
+    for (int j = 0; j < kPiNZ; ++j) {
+      if (!((walking >> j) & 1u) || v > amid[j]) continue;
+      const float t = tval(w, zc[j], v);
+      if (t > pitch / 4 || t < -pitch / 4) {
+        walking &= ~(1u << j);
+        amin[j] = v;
+        continue;
+      }
+      const float it = t * 2 * (A.nt - 1) / pitch + A.wt;
+      sum[j] += sample_rows<INTERP, ADDR>(w.view, A.ns, A.nt, w.c, it);
+    }
   }
-  const int a_min = ia;
-  // the reference has no bound against n_angle here (:225); views past the end sample
-  // outside the array, which border addressing reads as 0
-  for (ia = a_middle + 1; ia <= a_min + A.half && ia < A.n_angle; ++ia) {
-    bool stop = false;
-    sum += contrib(ia, stop, false);
+  // forward: views a_middle + 1 .. a_min + half (the reference has no bound against n_angle,
+  // :225; views past the end would sample outside the array, which reads as 0 -- left out)
+  int vlo = INT_MAX, vhi = -1;
+#pragma unroll
+  for (int j = 0; j < kPiNZ; ++j)
+    if (j < nzc) {
+      vlo = min(vlo, amid[j] + 1);
+      vhi = max(vhi, min(amin[j] + A.half, A.n_angle - 1));
+    }
+  for (int v = vlo; v <= vhi; ++v) {
+    const ViewTerms w = terms(v);
+#pragma unroll
+    for (int j = 0; j < kPiNZ; ++j) {
+      if (j >= nzc || v < amid[j] + 1 || v > amin[j] + A.half) continue;
+      const float t = tval(w, zc[j], v);
+      const float it = t * 2 * (A.nt - 1) / pitch + A.wt;
+      sum[j] += sample_rows<INTERP, ADDR>(w.view, A.ns, A.nt, w.c, it);
+    }
   }
-  A.img[((long long)iz * A.ny + iy) * A.nx + ix] = (float)((double)sum * kRefPi / A.half);
+#pragma unroll
+  for (int j = 0; j < kPiNZ; ++j)
+    if (j < nzc)
+      A.img[((long long)(z0 + j) * A.ny + iy) * A.nx + ix] = (float)((double)sum[j] * kRefPi / A.half);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -585,17 +633,17 @@ LCT_API int lct_backproject_pi_ori(const lct_geom* g, const lct_img* ig, const f
   a.betas = d_betas;
   a.img = d_img;
   a.nz = ig->nz;
-  dim3 grid((ig->nx + kBpTX - 1) / kBpTX, (ig->ny + kBpTY - 1) / kBpTY, ig->nz);
+  dim3 grid((ig->nx + kBpTX - 1) / kBpTX, (ig->ny + kBpTY - 1) / kBpTY, (ig->nz + kPiNZ - 1) / kPiNZ);
   dim3 block(kBpTX, kBpTY);
   cudaStream_t s = (cudaStream_t)stream;
   bool tex = interp == LCT_INTERP_TEX8, clamp = addr == LCT_ADDR_CLAMP;
   if (tex && clamp)
-    bp_pi_ori_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, block, 0, s>>>(a);
+    bp_pi_ori_z_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, block, 0, s>>>(a);
   else if (tex)
-    bp_pi_ori_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, block, 0, s>>>(a);
+    bp_pi_ori_z_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, block, 0, s>>>(a);
   else if (clamp)
-    bp_pi_ori_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, block, 0, s>>>(a);
+    bp_pi_ori_z_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, block, 0, s>>>(a);
   else
-    bp_pi_ori_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, block, 0, s>>>(a);
+    bp_pi_ori_z_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, block, 0, s>>>(a);
   return launch_status();
 }

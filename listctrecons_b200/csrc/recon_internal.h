@@ -87,12 +87,11 @@ int recon_setup(const lct_plan* plan, const lct_recon_opts* opts, lct_recon** ou
 int recon_alloc_common(lct_recon* r, const lct_plan* plan);
 int recon_alloc_status(int st);
 
-// the sampler a recon's options select: texture for TEX8 (AUTO or TEXTURE) when the windows
-// are full and the addressing is one mode for every slab; else quads
+// the texture sampler when asked for (TEX8, full windows, one addressing mode for every slab);
+// AUTO is quads, which measured faster on B200 for TEX8 too
 inline bool want_texture(const lct_recon_opts& o, bool full_windows) {
   return full_windows && o.backprojector == LCT_BP_PAR && o.interp == LCT_INTERP_TEX8 &&
-         o.addr != LCT_ADDR_LEGACY &&
-         (o.bp_sampler == LCT_BP_SAMPLER_AUTO || o.bp_sampler == LCT_BP_SAMPLER_TEXTURE);
+         o.addr != LCT_ADDR_LEGACY && o.bp_sampler == LCT_BP_SAMPLER_TEXTURE;
 }
 // the filtered views [v0, v0 + nv) (at par) into the backprojector's input: texture slots or
 // quads, ring-aware (bounded recons)

@@ -25,22 +25,30 @@ __global__ void tex3d_sample_kernel(cudaTextureObject_t tex, const float* __rest
 }
 
 // Every CTA re-reads one 16 KiB buffer (resident in each SM's L1 after the first pass): each warp
-// instruction is one LDG.128 of 512 contiguous bytes, eight independent loads per unrolled step.
+// instruction is one LDG.128 of 512 contiguous, aligned bytes, eight independent loads per
+// unrolled step, the step's window moving by one warp row each iteration.  The loads are volatile
+// asm (ld.global.nc.v4.f32, the non-coherent path __ldg takes), so none is hoisted or merged.
 constexpr int kL1Vec = 1024;  // float4 in the buffer (16 KiB)
+__device__ __forceinline__ float4 ldg128_volatile(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "l"(p));
+  return v;
+}
 __global__ void __launch_bounds__(256) l1_load_kernel(const float4* __restrict__ buf, int iters,
                                                       float* __restrict__ sink) {
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  int i = threadIdx.x;
   for (int it = 0; it < iters; it += 8) {
+    const int base = (int)threadIdx.x + 32 * (it >> 3);
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const float4 v = __ldg(buf + ((i + u * 256) & (kL1Vec - 1)));
+      const float4 v = ldg128_volatile(buf + ((base + u * 256) & (kL1Vec - 1)));
       acc.x += v.x;
       acc.y += v.y;
       acc.z += v.z;
       acc.w += v.w;
     }
-    i = (i + 8 * 256) & (kL1Vec - 1);
   }
   // the buffer is zero, so nothing is written; the compiler cannot know that
   if (acc.x + acc.y + acc.z + acc.w != 0.f) sink[blockIdx.x * blockDim.x + threadIdx.x] = acc.x;
