@@ -314,12 +314,12 @@ int lct_recon_create_bounded(const lct_plan* plan, const lct_recon_opts* opts, i
 int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
 /* Whole scan from the reference's raw files: RawDataReader::readData (Src/DataReader.cpp:8-19)
    and RawImageWriter (Src/ImageWriter.cpp:9-43) for every block of the run, with 64-bit offsets.
-   fan_path: the DataInterpFile, fan view v of the scan at byte (v + DataOffset) * nt * ns * 4; a
-   reader thread reads the run's views into pinned chunks that are uploaded as the pipeline
+   fan_path: the DataInterpFile, fan view v of the scan at byte (v + DataOffset) * nt * ns * 4;
+   three reader threads read the run's views into pinned chunks that are uploaded as the pipeline
    needs them.  image_path (or NULL): the volume [n_blocks_run * 32][ny][nx] float32 is written
    there slab by slab by a writer thread; image (or NULL): host buffer for the volume.  At least
    one of the two.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
-   correction.  The first call allocates the recon's pinned staging (three fan chunks, two slabs),
+   correction.  The first call allocates the recon's pinned staging (six fan chunks, two slabs),
    kept until lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
 int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,
                        lct_stream stream);

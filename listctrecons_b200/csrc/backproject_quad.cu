@@ -294,6 +294,7 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
     vhi = min(vhi, A.view_hi);
   }
   const int sv = A.slab_view[slab];
+  const float4* quads = A.quads + (long long)sv * A.qstride;  // linear buffers: slab's view 0
   const float* betas = A.betas + sv;
   const float wt = A.wt;
 
@@ -315,8 +316,9 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       view_trig_pi(betas, ia, c1, s1);
       view_trig_pi(betas, ia + A.half, c2, s2);
       s_cs[tid] = make_float4(c1, s1, c2, s2);
-      const float4* v1 = quad_view_ptr(A, sv, ia);
-      const float4* v2 = quad_view_ptr(A, sv, ia + A.half);
+      const float4* v1 = A.qring > 0 ? quad_view_ptr(A, sv, ia) : quads + (long long)ia * A.qstride;
+      const float4* v2 = A.qring > 0 ? quad_view_ptr(A, sv, ia + A.half)
+                                     : quads + (long long)(ia + A.half) * A.qstride;
       if (INTERP != LCT_INTERP_EXACT)
         s_qv[tid] = make_ulonglong2(reinterpret_cast<unsigned long long>(v1),
                                     reinterpret_cast<unsigned long long>(v2));

@@ -47,7 +47,8 @@ namespace lct {
 
 constexpr long long kDefaultPiece = 512;  // views per rebin / filter / pack step
 constexpr int kImgRing = 4;               // slabs in the volume ring (host / file output)
-constexpr int kFanStage = 3;              // pinned fan chunks of lct_recon_run_file
+constexpr int kFanStage = 6;              // pinned fan chunks of lct_recon_run_file
+constexpr int kFanReaders = 3;            // reader threads (chunk c on thread c mod 3)
 constexpr int kImgStage = 2;              // pinned slabs of the file writer
 
 // Fan views a global parallel view g reads lie in [g + lo, g + hi] (scan rebin shifts, FP64).
@@ -60,7 +61,7 @@ static void rebin_reach(const lct_geom& g, long long& lo, long long& hi) {
 }
 
 // ----------------------------------------------------------------------------------------------
-// reader: file views -> pinned chunks (a thread), chunks -> device (the issuing thread)
+// reader: file views -> pinned chunks (kFanReaders threads), chunks -> device (the issuing thread)
 // ----------------------------------------------------------------------------------------------
 class FanReader {
  public:
@@ -82,10 +83,11 @@ class FanReader {
     stage_ = stage;
     slots_ = slots;
     state_.assign(slots, kFree);
-    held_.assign(slots, -1);
+    held_.resize(slots);
+    for (int i = 0; i < slots; ++i) held_[i] = i - slots;  // "chunk i - slots" done: free for chunk i
     rel_.resize(slots);
     for (int i = 0; i < slots; ++i) rel_[i] = {this, i};
-    th_ = std::thread([this] { loop(); });
+    for (int t = 0; t < kFanReaders; ++t) th_.emplace_back([this, t] { loop(t); });
     return LCT_OK;
   }
   long long chunks() const { return (nviews_ + chunk_ - 1) / chunk_; }
@@ -115,7 +117,9 @@ class FanReader {
       stop_ = true;
     }
     cv_.notify_all();
-    if (th_.joinable()) th_.join();
+    for (auto& t : th_)
+      if (t.joinable()) t.join();
+    th_.clear();
     if (fd_ >= 0) ::close(fd_);
     fd_ = -1;
     return err_;
@@ -135,13 +139,17 @@ class FanReader {
     }
     r->self->cv_.notify_all();
   }
-  void loop() {
-    for (long long c = 0; c < chunks(); ++c) {
+  // reader thread t: chunks t, t + kFanReaders, ...; chunk c waits for its slot (c mod slots)
+  // to be free, i.e. for chunk c - slots to be uploaded
+  void loop(int t) {
+    for (long long c = t; c < chunks(); c += kFanReaders) {
       const int slot = (int)(c % slots_);
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_.wait(lk, [&] { return stop_ || state_[slot] == kFree; });
-        if (stop_) return;
+        cv_.wait(lk, [&] {
+          return stop_ || err_ || (state_[slot] == kFree && held_[slot] == c - slots_);
+        });
+        if (stop_ || err_) return;
         state_[slot] = kReading;
       }
       const long long nv = std::min(chunk_, nviews_ - c * chunk_);
@@ -176,7 +184,7 @@ class FanReader {
   std::vector<int> state_;
   std::vector<long long> held_;
   std::vector<Rel> rel_;
-  std::thread th_;
+  std::vector<std::thread> th_;
   std::mutex mu_;
   std::condition_variable cv_;
   bool stop_ = false;
