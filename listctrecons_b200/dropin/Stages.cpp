@@ -15,7 +15,8 @@
 // Sampling: the reference's texture semantics (LCT_INTERP_TEX8) with the legacy binding
 // behaviour of its texture references (Clamp for the first bound block, Border afterwards:
 // LCT_ADDR_LEGACY).  Environment switches: LCT_DROPIN_ADDR=border|clamp|legacy,
-// LCT_DROPIN_INTERP=tex8|exact, LCT_DROPIN_FILTER=fp32|bf16x3|bf16x6.
+// LCT_DROPIN_INTERP=tex8|exact, LCT_DROPIN_FILTER=fp32|bf16x3|bf16x6,
+// LCT_DROPIN_FILTERED_COPY=0 (skip the filtered block's copy to host `rebin`).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -203,7 +204,12 @@ void Filter::filter(const ReconData* mr) {
                           nullptr),
           "lct_filter_rows"))
     return;
-  dg->proj_gpu()->copy_to_CPU(mr->data_cpu()->rebin_(), (size_t)ns * ctg->nt_() * ctg->n_angle());
+  // the reference copies every filtered block to host `rebin` (CUDA/Filter.cu:69), which only its
+  // writer's rebin.raw dump reads; LCT_DROPIN_FILTERED_COPY=0 skips that copy (rebin.raw then
+  // holds zeros)
+  const char* keep = std::getenv("LCT_DROPIN_FILTERED_COPY");
+  if (!keep || std::strcmp(keep, "0") != 0)
+    dg->proj_gpu()->copy_to_CPU(mr->data_cpu()->rebin_(), (size_t)ns * ctg->nt_() * ctg->n_angle());
   std::cout << "Filter finished" << std::endl;
 }
 
