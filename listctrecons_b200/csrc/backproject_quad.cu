@@ -247,7 +247,7 @@ __device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a
 
 // One tile: voxel columns [bx*32, +32) x [by*8, +8), slab/slice chunk bz.  Called with
 // CTA-uniform arguments by every thread of a 256-thread CTA.
-template <int NZ, int INTERP, bool PART>
+template <int NZ, int INTERP, bool PART, bool RING>
 __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by, int bz) {
   __shared__ float4 s_cs[kQVB];      // cos, sin of view ia and of its conjugate ia + half
   __shared__ int2 s_jr[kQVB];        // slices [jlo, jhi) of the chunk whose window holds ia
@@ -316,9 +316,9 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
       view_trig_pi(betas, ia, c1, s1);
       view_trig_pi(betas, ia + A.half, c2, s2);
       s_cs[tid] = make_float4(c1, s1, c2, s2);
-      const float4* v1 = A.qring > 0 ? quad_view_ptr(A, sv, ia) : quads + (long long)ia * A.qstride;
-      const float4* v2 = A.qring > 0 ? quad_view_ptr(A, sv, ia + A.half)
-                                     : quads + (long long)(ia + A.half) * A.qstride;
+      const float4* v1 = RING ? quad_view_ptr(A, sv, ia) : quads + (long long)ia * A.qstride;
+      const float4* v2 = RING ? quad_view_ptr(A, sv, ia + A.half)
+                              : quads + (long long)(ia + A.half) * A.qstride;
       if (INTERP != LCT_INTERP_EXACT)
         s_qv[tid] = make_ulonglong2(reinterpret_cast<unsigned long long>(v1),
                                     reinterpret_cast<unsigned long long>(v2));
@@ -491,10 +491,11 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
 }
 
 // PART: a view range of the slabs with raw sums carried in img (BpLaunch::part); the whole-
-// launch instantiation has none of that code
-template <int NZ, int INTERP, int MINB, bool PART>
+// launch instantiation has none of that code.  RING: the quads are a ring (bounded recons); the
+// linear instantiation has no modulo in its view bases.
+template <int NZ, int INTERP, int MINB, bool PART, bool RING>
 __global__ void __launch_bounds__(kQTX* kQTY, MINB) bp_quad_kernel(const __grid_constant__ BpQuadArgs A) {
-  bp_quad_tile<NZ, INTERP, PART>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+  bp_quad_tile<NZ, INTERP, PART, RING>(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // EXACT with every view's tile footprint staged in shared memory by TMA.  Per view pair the
@@ -948,7 +949,7 @@ __global__ void __launch_bounds__(kQTX* kQTY, MINB)
     const int bx = local % sA.gx;
     const int by = (local / sA.gx) % sA.gy;
     const int bz = local / (sA.gx * sA.gy);
-    bp_quad_tile<NZ, INTERP, false>(sA, bx, by, bz);
+    bp_quad_tile<NZ, INTERP, false, false>(sA, bx, by, bz);
   }
 }
 
@@ -1037,13 +1038,30 @@ int launch_bp_par_quads(const lct_geom& g, const lct_img& ig, const BpLaunch& L,
   int minb = L.minb;
   if (minb < 1 || minb > 4) minb = 4;  // measured best on B200 (4 CTAs x 256 threads per SM)
   const bool part = L.part != kBpWhole || L.view_lo > 0 || L.view_hi < (1 << 30);
-#define LCT_BPQ(NZV, MB)                                                                      \
-  do {                                                                                        \
-    if (part && tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB, true><<<grid, block, 0, s>>>(a);  \
-    else if (part) bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB, true><<<grid, block, 0, s>>>(a);   \
-    else if (tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB, false><<<grid, block, 0, s>>>(a);    \
-    else bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB, false><<<grid, block, 0, s>>>(a);            \
+#define LCT_BPQ(NZV, MB)                                                                          \
+  do {                                                                                            \
+    if (part && tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB, true, false><<<grid, block, 0, s>>>(a); \
+    else if (part) bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB, true, false><<<grid, block, 0, s>>>(a);  \
+    else if (tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, MB, false, false><<<grid, block, 0, s>>>(a);   \
+    else bp_quad_kernel<NZV, LCT_INTERP_EXACT, MB, false, false><<<grid, block, 0, s>>>(a);           \
   } while (0)
+  // quad rings (bounded recons): 4 CTAs per SM
+#define LCT_BPQR(NZV)                                                                            \
+  do {                                                                                           \
+    if (part && tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, 4, true, true><<<grid, block, 0, s>>>(a); \
+    else if (part) bp_quad_kernel<NZV, LCT_INTERP_EXACT, 4, true, true><<<grid, block, 0, s>>>(a);  \
+    else if (tex) bp_quad_kernel<NZV, LCT_INTERP_TEX8, 4, false, true><<<grid, block, 0, s>>>(a);   \
+    else bp_quad_kernel<NZV, LCT_INTERP_EXACT, 4, false, true><<<grid, block, 0, s>>>(a);           \
+  } while (0)
+  if (a.qring > 0) {
+    switch (nzt) {
+      case 4: LCT_BPQR(4); break;
+      case 16: LCT_BPQR(16); break;
+      default: LCT_BPQR(8);
+    }
+#undef LCT_BPQR
+    return launch_status();
+  }
 #define LCT_BPQ_NZ(NZV)            \
   do {                             \
     switch (minb) {                \
