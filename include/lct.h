@@ -105,7 +105,9 @@ int lct_rebin_fan2par_scan(const lct_geom* g, const float* d_fan, int64_t fan_fi
 /* NullRebinerGPU::rebin + rebin_null_kernel (CUDA/Rebiner.cu:13-80) */
 int lct_rebin_null(const lct_geom* g, const float* d_fan, float* d_par, int addr,
                    lct_stream stream);
-/* PiOriRebiner::rebin + rebin_pi_ori_kernel (CUDA/Rebiner.cu:156-233) */
+/* PiOriRebiner::rebin + rebin_pi_ori_kernel (CUDA/Rebiner.cu:156-233).  TEX8 samples the fan
+   block through the texture unit as the reference does (its trilinear filter, a 3-D array bound
+   for the call) and therefore synchronises the stream before returning; EXACT is asynchronous. */
 int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par, int interp, int addr,
                      lct_stream stream);
 

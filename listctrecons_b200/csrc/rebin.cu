@@ -437,6 +437,26 @@ LCT_API int lct_rebin_null(const lct_geom* g, const float* d_fan, float* d_par, 
   return launch_status();
 }
 
+// TEX8 PI-original rebin through the texture unit, as the reference samples it
+// (CUDA/Rebiner.cu:156-179): all three coordinates off texel centres, so the unit's trilinear
+// filter -- which register emulation matches only to within two 8-bit weight steps -- is used
+// itself.  Coordinates as in rebin_pi_ori_kernel's TEX8 branch.
+__global__ void __launch_bounds__(256) rebin_pi_ori_tex_kernel(cudaTextureObject_t tex,
+                                                               float* __restrict__ par, RebinArgs a) {
+  const int ia = blockIdx.x, it = blockIdx.y;
+  for (int is = threadIdx.x; is < a.ns; is += blockDim.x) {
+    float s = (is - a.ws) * a.ds;
+    float gamma = asinf(s / a.dso);
+    float pidx = gamma * a.dso / a.ds + a.ws;
+    double num = (double)((it - a.wt) * a.pitch / (float)(2 * (a.nt - 1))) -
+                 (double)(gamma * a.pitch) / (2 * kRefPi);
+    float q = (float)(num / (double)cosf(gamma));
+    float qidx = q / a.dt + a.wt;
+    float bidx = ia + gamma / a.orbit + (float)a.add;
+    par[((long long)ia * a.nt + it) * a.ns + is] = tex3D<float>(tex, pidx + 0.5f, qidx + 0.5f, bidx + 0.5f);
+  }
+}
+
 LCT_API int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par, int interp,
                              int addr, lct_stream stream) {
   int st = check_geom(g);
@@ -447,11 +467,21 @@ LCT_API int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par
   dim3 grid(g->n_angle, g->nt);
   cudaStream_t s = (cudaStream_t)stream;
   bool tex = interp == LCT_INTERP_TEX8, clamp = addr == LCT_ADDR_CLAMP;
-  if (tex && clamp)
-    rebin_pi_ori_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, d_par, a);
-  else if (tex)
-    rebin_pi_ori_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, d_par, a);
-  else if (clamp)
+  if (tex) {
+    // the fan block as a 3-D texture for the call (the reference binds it per block too,
+    // CUDA/Rebiner.cu:181-230); released after the kernel, so this mode synchronises the stream
+    ViewTexture t;
+    if ((st = view_texture_create(t, g->ns, g->nt, g->n_angle_add, addr))) return st;
+    st = view_texture_fill(t, d_fan, g->n_angle_add, 0, s);
+    if (!st) {
+      rebin_pi_ori_tex_kernel<<<grid, 256, 0, s>>>(t.tex, d_par, a);
+      st = launch_status();
+    }
+    const int st2 = cuda_status(cudaStreamSynchronize(s));
+    view_texture_destroy(t);
+    return st ? st : st2;
+  }
+  if (clamp)
     rebin_pi_ori_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, 256, 0, s>>>(d_fan, d_par, a);
   else
     rebin_pi_ori_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, 256, 0, s>>>(d_fan, d_par, a);
