@@ -32,6 +32,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -382,6 +383,11 @@ def plain_gpu(w, geo, ph, ours_value):
             secs = rec["reconstruct_seconds"] * w["blocks"] / rec["n_blocks"]
             runs[name] = {"value": upd / secs / 1e9, "unit": UNIT, "s_per_volume": secs,
                           "blocks_timed": rec["n_blocks"]}
+            m = re.search(r"\[B200\] create ([0-9.]+) s, run ([0-9.]+) s, destroy ([0-9.]+) s",
+                          r.stdout)
+            if m:  # the whole-scan type's split of reconstruct() (all blocks timed, unscaled)
+                runs[name]["split_s"] = dict(zip(("create", "run", "destroy"),
+                                                 map(float, m.groups())))
     out = runs.pop("reference")
     if "value" in out:
         out["speedup_e2e"] = ours_value / out["value"]

@@ -295,8 +295,10 @@ int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon
    Scan mode (fan->parallel rebin, no pre-weighting, parallel BP) with a HOST fan streams: fan
    views are uploaded in pieces on an internal copy stream while earlier pieces are rebinned,
    filtered and backprojected slab by slab, and each finished slab is downloaded on a second copy
-   stream (pinned host buffers make the copies asynchronous).  The volume is bit-identical to
-   the device-resident run. */
+   stream (pinned host buffers make the copies asynchronous; a pageable volume is downloaded
+   once after the pipeline, or, for a bounded recon, copied out of pinned slabs by two threads,
+   so the pipeline is never held by a copy into pageable memory).  The volume is bit-identical
+   to the device-resident run. */
 int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
                   float* image, int image_on_device, lct_stream stream);
 /* Bounded device memory (no reference counterpart for the bound; the reference bounds memory
@@ -317,12 +319,14 @@ int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
 /* Whole scan from the reference's raw files: RawDataReader::readData (Src/DataReader.cpp:8-19)
    and RawImageWriter (Src/ImageWriter.cpp:9-43) for every block of the run, with 64-bit offsets.
    fan_path: the DataInterpFile, fan view v of the scan at byte (v + DataOffset) * nt * ns * 4;
-   three reader threads read the run's views into pinned chunks that are uploaded as the pipeline
-   needs them.  image_path (or NULL): the volume [n_blocks_run * 32][ny][nx] float32 is written
-   there slab by slab by a writer thread; image (or NULL): host buffer for the volume.  At least
-   one of the two.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
-   correction.  The first call allocates the recon's pinned staging (six fan chunks, two slabs),
-   kept until lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
+   four reader threads read the run's views into pinned chunks (whole views, at most 16 MiB)
+   that are uploaded as the pipeline needs them.  image_path (or NULL): the volume [n_blocks_run * 32][ny][nx] float32 is written
+   there slab by slab; image (or NULL): host buffer for the volume, pinned or pageable.  At least
+   one of the two.  A file, or a pageable buffer, is written from pinned slabs by two writer
+   threads (both outputs from one download per slab); a pinned buffer alone is downloaded into
+   directly.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
+   correction.  The first call allocates the recon's pinned staging (eight fan chunks, three
+   slabs), kept until lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
 int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,
                        lct_stream stream);
 /* Backprojection autotuner (no reference counterpart): times the kernel's slices-per-thread x

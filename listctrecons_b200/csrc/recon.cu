@@ -753,10 +753,18 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     }
     // the other streams start after everything already queued on s (an earlier run included)
     if ((st = streams_fork(r->ss, s, r->sev[0]))) return st;
-    if ((st = recon_run_streamed(r, fan, skip, d_img, d_out, image_on_device ? nullptr : image, s,
+    // a pageable volume is downloaded once, after the pipeline: slab downloads into it would each
+    // hold this thread until the slab is backprojected
+    const bool host_slabs = !image_on_device && host_pinned(image);
+    if ((st = recon_run_streamed(r, fan, skip, d_img, d_out, host_slabs ? image : nullptr, s,
                                  r->ss)))
       return st;
     if ((st = streams_join(r->ss, s, r->sev.data() + 1))) return st;
+    if (!image_on_device && !host_slabs &&
+        (st = cuda_status(cudaMemcpyAsync(image, d_out, sizeof(float) * nb * kBlockSlices *
+                                                            (long long)ig.nx * ig.ny,
+                                          cudaMemcpyDeviceToHost, s))))
+      return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[4], s)))) return st;
     if ((st = cuda_status(cudaEventRecord(r->ev[5], s)))) return st;
     if ((st = cuda_status(cudaEventSynchronize(r->ev[5])))) return st;

@@ -18,9 +18,9 @@
 // the first in parts while its window arrives, exactly as the streamed unbounded run does; the
 // kernels and their order per view are the same, so the volume is bit-identical to it.
 //
-// lct_recon_run_file reads the fan from the reference's raw file with 64-bit offsets on a reader
-// thread into pinned chunks that are uploaded as the pipeline needs them, and writes the volume
-// through a slab writer thread (64-bit offsets) -- RawDataReader::readData and RawImageWriter
+// lct_recon_run_file reads the fan from the reference's raw file with 64-bit offsets on reader
+// threads into small pinned chunks that are uploaded as the pipeline needs them, and writes the
+// volume through slab writer threads (64-bit offsets) -- RawDataReader::readData and RawImageWriter
 // (Src/ImageWriter.cpp:9-43) for whole scans.
 #include <fcntl.h>
 #include <sys/stat.h>
@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cerrno>
 #include <cmath>
+#include <cstring>
 #include <condition_variable>
 #include <mutex>
 #include <new>
@@ -47,9 +48,11 @@ namespace lct {
 
 constexpr long long kDefaultPiece = 512;  // views per rebin / filter / pack step
 constexpr int kImgRing = 4;               // slabs in the volume ring (host / file output)
-constexpr int kFanStage = 6;              // pinned fan chunks of lct_recon_run_file
-constexpr int kFanReaders = 3;            // reader threads (chunk c on thread c mod 3)
-constexpr int kImgStage = 2;              // pinned slabs of the file writer
+constexpr int kFanStage = 8;              // pinned fan chunks of lct_recon_run_file
+constexpr long long kFanChunkBytes = 16LL << 20;  // a chunk: whole views, at most 16 MiB (>= 1 view)
+constexpr int kFanReaders = 4;            // reader threads (chunk c on thread c mod 4)
+constexpr int kImgStage = 3;              // pinned slabs of the slab writer
+constexpr int kSinkThreads = 2;           // slab writer threads (file writes, pageable copies)
 
 // Fan views a global parallel view g reads lie in [g + lo, g + hi] (scan rebin shifts, FP64).
 static void rebin_reach(const lct_geom& g, long long& lo, long long& hi) {
@@ -91,6 +94,7 @@ class FanReader {
     return LCT_OK;
   }
   long long chunks() const { return (nviews_ + chunk_ - 1) / chunk_; }
+  long long chunk() const { return chunk_; }
   // blocks until chunk c is in its pinned slot
   int acquire(long long c, const float** data, long long* nv) {
     const int slot = (int)(c % slots_);
@@ -192,18 +196,26 @@ class FanReader {
 };
 
 // ----------------------------------------------------------------------------------------------
-// writer: device slab -> pinned slot (D2H on the download stream) -> file (a thread)
+// writer: device slab -> pinned slot (D2H on the download stream) -> file and/or pageable host
+// volume (two threads)
 // ----------------------------------------------------------------------------------------------
 class SlabWriter {
  public:
-  int start(const char* path, long long slab_bytes, int nslabs, float* stage, int slots) {
-    fd_ = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
-    if (fd_ < 0) return LCT_ERR_IO;
-    if (::ftruncate(fd_, (off_t)(slab_bytes * nslabs)) != 0) {
-      ::close(fd_);
-      fd_ = -1;
-      return LCT_ERR_IO;
+  // path (or null): the volume file, sized and written slab by slab; host (or null): a pageable
+  // host volume the slabs are copied into (a download straight into pageable memory would hold
+  // the issuing thread until the slab is backprojected, stalling the whole pipeline)
+  int start(const char* path, float* host, long long slab_bytes, int nslabs, float* stage,
+            int slots) {
+    if (path) {
+      fd_ = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+      if (fd_ < 0) return LCT_ERR_IO;
+      if (::ftruncate(fd_, (off_t)(slab_bytes * nslabs)) != 0) {
+        ::close(fd_);
+        fd_ = -1;
+        return LCT_ERR_IO;
+      }
     }
+    host_ = reinterpret_cast<char*>(host);
     slab_bytes_ = slab_bytes;
     stage_ = stage;
     slots_ = slots;
@@ -211,7 +223,7 @@ class SlabWriter {
     dest_.assign(slots, -1);
     sub_.resize(slots);
     for (int i = 0; i < slots; ++i) sub_[i] = {this, i};
-    th_ = std::thread([this] { loop(); });
+    for (int t = 0; t < kSinkThreads; ++t) th_.emplace_back([this] { loop(); });
     return LCT_OK;
   }
   // pinned slot for the k-th slab written (blocks while its previous slab is being written)
@@ -246,7 +258,9 @@ class SlabWriter {
       stop_ = true;
     }
     cv_.notify_all();
-    if (th_.joinable()) th_.join();
+    for (std::thread& t : th_)
+      if (t.joinable()) t.join();
+    th_.clear();
     if (fd_ >= 0 && ::close(fd_) != 0 && !err_) err_ = LCT_ERR_IO;
     fd_ = -1;
     return err_;
@@ -276,7 +290,9 @@ class SlabWriter {
         ready_.erase(ready_.begin());
       }
       const char* src = reinterpret_cast<const char*>(stage_) + (long long)slot * slab_bytes_;
-      long long left = slab_bytes_, off = (long long)dest_[slot] * slab_bytes_;
+      const long long off0 = (long long)dest_[slot] * slab_bytes_;
+      if (host_) std::memcpy(host_ + off0, src, (size_t)slab_bytes_);
+      long long left = fd_ >= 0 ? slab_bytes_ : 0, off = off0;
       int e = LCT_OK;
       while (left > 0) {
         const ssize_t n = ::pwrite(fd_, src, (size_t)std::min<long long>(left, 1LL << 30), (off_t)off);
@@ -298,12 +314,13 @@ class SlabWriter {
     }
   }
   int fd_ = -1;
+  char* host_ = nullptr;
   long long slab_bytes_ = 0;
   float* stage_ = nullptr;
   int slots_ = 0;
   std::vector<int> busy_, dest_, ready_;
   std::vector<Sub> sub_;
-  std::thread th_;
+  std::vector<std::thread> th_;
   std::mutex mu_;
   std::condition_variable cv_;
   bool stop_ = false;
@@ -421,9 +438,10 @@ static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink
           while (up < need) {  // whole chunks, in order
             const float* h = nullptr;
             long long nv = 0;
-            if ((st = feed.reader->acquire(up / P, &h, &nv))) return st;
+            const long long c = up / feed.reader->chunk();
+            if ((st = feed.reader->acquire(c, &h, &nv))) return st;
             if ((st = upload(up, up + nv, h))) return st;
-            if ((st = feed.reader->release_after(ss.up, up / P))) return st;
+            if ((st = feed.reader->release_after(ss.up, c))) return st;
             up += nv;
           }
         } else {
@@ -532,6 +550,25 @@ static int run_forked(lct_recon* r, cudaStream_t s, F body) {
   return LCT_OK;
 }
 
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// the slab writer's pinned slots, allocated on first use and kept with the recon
+static int ensure_img_stage(lct_recon* r, long long slab) {
+  if (r->h_img_stage) return LCT_OK;
+  int st = cuda_status(cudaHostAlloc((void**)&r->h_img_stage, sizeof(float) * kImgStage * slab,
+                                     cudaHostAllocDefault));
+  if (st) return recon_alloc_status(st);
+  r->img_stage_slots = kImgStage;
+  return LCT_OK;
+}
+
 int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, float* image,
                           bool image_on_device, cudaStream_t s) {
   FanFeed feed;
@@ -540,10 +577,25 @@ int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, fl
     feed.dev = fan;
   else
     feed.host = fan;
-  if (image_on_device)
+  if (image_on_device) {
     sink.dev = image;
-  else
+  } else if (host_pinned(image)) {
     sink.host = image;
+  } else {
+    // pageable volume: slabs go through the pinned slots and are copied on the writer's threads
+    const lct_img& ig = r->info.ig;
+    const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
+    int st = ensure_img_stage(r, slab);
+    if (st) return st;
+    SlabWriter writer;
+    if ((st = writer.start(nullptr, image, (long long)sizeof(float) * slab, r->info.n_blocks_run,
+                           r->h_img_stage, r->img_stage_slots)))
+      return st;
+    sink.writer = &writer;
+    st = run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
+    const int st_w = writer.finish();
+    return st ? st : st_w;
+  }
   return run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
 }
 
@@ -643,30 +695,30 @@ LCT_API int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* i
   const long long P = r->piece > 0 ? r->piece : kDefaultPiece;
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
   int st;
-  // pinned staging, allocated on the first call and kept with the recon
+  // pinned staging, allocated on the first call and kept with the recon: chunks of whole views
+  // (pinning costs time in proportion to the bytes, so the chunks are small and many)
+  const long long view_bytes = (long long)sizeof(float) * r->plane;
+  const long long chunk = std::max<long long>(1, std::min<long long>(P, kFanChunkBytes / view_bytes));
   if (!r->h_fan_stage) {
     if ((st = cuda_status(cudaHostAlloc((void**)&r->h_fan_stage,
-                                        sizeof(float) * kFanStage * P * r->plane,
+                                        sizeof(float) * kFanStage * chunk * r->plane,
                                         cudaHostAllocDefault))))
       return recon_alloc_status(st);
     r->fan_stage_slots = kFanStage;
   }
-  if (image_path && !r->h_img_stage) {
-    if ((st = cuda_status(cudaHostAlloc((void**)&r->h_img_stage, sizeof(float) * kImgStage * slab,
-                                        cudaHostAllocDefault))))
-      return recon_alloc_status(st);
-    r->img_stage_slots = kImgStage;
-  }
+  // a file, or a pageable volume, is written from pinned slots by the writer's threads (both at
+  // once when both are asked for); a pinned volume is downloaded into directly
+  const bool use_writer = image_path || !host_pinned(image);
+  if (use_writer && (st = ensure_img_stage(r, slab))) return st;
   FanReader reader;
   SlabWriter writer;
   // file view v of the run's fan views lies at (fan_first + DataOffset + v) views into the file
   // (Src/DataReader.cpp:14, in 64 bits)
-  const long long view_bytes = (long long)sizeof(float) * r->plane;
   const long long byte0 = (r->fan_first + r->info.data_offset) * view_bytes;
-  if ((st = reader.start(fan_path, byte0, view_bytes, r->fan_count, P, r->h_fan_stage,
+  if ((st = reader.start(fan_path, byte0, view_bytes, r->fan_count, chunk, r->h_fan_stage,
                          r->fan_stage_slots)))
     return st;
-  if (image_path && (st = writer.start(image_path, (long long)sizeof(float) * slab, nb,
+  if (use_writer && (st = writer.start(image_path, image, (long long)sizeof(float) * slab, nb,
                                        r->h_img_stage, r->img_stage_slots))) {
     reader.finish();
     return st;
@@ -674,32 +726,12 @@ LCT_API int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* i
   FanFeed feed;
   feed.reader = &reader;
   ImageSink sink;
-  sink.host = image;
-  sink.writer = image_path ? &writer : nullptr;
-  if (image && image_path) {
-    // one download per slab: the file is written from the caller's buffer's copy as well
-    sink.host = nullptr;
-  }
+  if (use_writer)
+    sink.writer = &writer;
+  else
+    sink.host = image;
   st = run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
   const int st_r = reader.finish();
-  const int st_w = image_path ? writer.finish() : LCT_OK;
-  if (!st && image && image_path) {
-    // the caller also wants the volume in memory: read back what the writer wrote
-    const int fd = ::open(image_path, O_RDONLY);
-    if (fd < 0) return LCT_ERR_IO;
-    char* dst = reinterpret_cast<char*>(image);
-    long long left = (long long)sizeof(float) * slab * nb, off = 0;
-    while (left > 0) {
-      const ssize_t n = ::pread(fd, dst, (size_t)std::min<long long>(left, 1LL << 30), (off_t)off);
-      if (n <= 0) {
-        ::close(fd);
-        return LCT_ERR_IO;
-      }
-      dst += n;
-      off += n;
-      left -= n;
-    }
-    ::close(fd);
-  }
+  const int st_w = use_writer ? writer.finish() : LCT_OK;
   return st ? st : (st_r ? st_r : st_w);
 }

@@ -115,6 +115,10 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
 int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, float* image,
                           bool image_on_device, cudaStream_t s);
 void recon_free_bounded(lct_recon* r);  // pinned staging of lct_recon_run_file
+// True for host memory the driver has pinned (cudaHostAlloc, cudaHostRegister): copies to it are
+// asynchronous.  A copy to pageable memory returns only once it is done, holding the thread that
+// queues the pipeline.
+bool host_pinned(const void* p);
 // learned correction of slices [z0, z1) of an nz-slice volume (cnn.cu)
 int cnn_infer_range(lct_cnn* c, const float* d_vol, float* d_out, int nz, int z0, int z1,
                     float bound, cudaStream_t s);

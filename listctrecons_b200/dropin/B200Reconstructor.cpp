@@ -14,7 +14,8 @@
 //     reference's Filter copies to host `rebin` does not exist in this flow: `rebin` stays zero.
 //
 // Defaults: exact interpolation, the BF16x6 tensor-core filter, border addressing, a bounded
-// device footprint (lct_recon_create_bounded) fed by lct_recon_run_file's reader thread.
+// device footprint (lct_recon_create_bounded) fed by lct_recon_run_file's reader threads.  The
+// recon's create, run and destroy times are printed on one "[B200]" line.
 // Environment switches, as for the stage drop-in: LCT_DROPIN_INTERP=tex8|exact,
 // LCT_DROPIN_FILTER=fp32|bf16x3|bf16x6, LCT_DROPIN_ADDR=border|clamp|legacy.  LEGACY (the
 // reference's clamped first block) needs the whole filtered views on the device: that run
@@ -181,10 +182,16 @@ void B200FDKReconstructor::reconstruct(const ReconData* mr) {
   const std::string path = mr->fi_()->in_file_dir() + mr->fi_()->data_file_name();
   float* image = mr->data_cpu()->image_();
   lct_recon* r = nullptr;
+  using clk = std::chrono::steady_clock;
+  const clk::time_point t0 = clk::now();
+  clk::time_point t1 = t0;
   if (o.addr != LCT_ADDR_LEGACY) {
-    if (ok(lct_recon_create_bounded(plan, &o, 0, &r), "lct_recon_create_bounded"))
+    if (ok(lct_recon_create_bounded(plan, &o, 0, &r), "lct_recon_create_bounded")) {
+      t1 = clk::now();
       ok(lct_recon_run_file(r, path.c_str(), nullptr, image, nullptr), "lct_recon_run_file");
+    }
   } else if (ok(lct_recon_create(plan, &o, &r), "lct_recon_create")) {
+    t1 = clk::now();
     int64_t first = 0, count = 0;
     lct_recon_fan_range(r, &first, &count);
     const long long view_bytes = (long long)sizeof(float) * ctg->ns_() * ctg->nt_();
@@ -198,8 +205,15 @@ void B200FDKReconstructor::reconstruct(const ReconData* mr) {
       ok(lct_recon_run(r, fan, first + info.data_offset, 0, image, 0, nullptr), "lct_recon_run");
     if (fan) cudaFreeHost(fan);
   }
+  const clk::time_point t2 = clk::now();
   if (r) lct_recon_destroy(r);
   lct_plan_destroy(plan);
+  const clk::time_point t3 = clk::now();
+  auto secs = [](clk::time_point a, clk::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+  };
+  std::printf("[B200] create %.4f s, run %.4f s, destroy %.4f s\n", secs(t0, t1), secs(t1, t2),
+              secs(t2, t3));
   std::cout << "Reconstruction of " << nb << " blocks finished." << std::endl;
 }
 

@@ -4,8 +4,8 @@ A bounded recon keeps fan, filtered and quad views in rings and the volume in a 
 a scan of six blocks with small pieces makes every ring wrap several times.  Each view is still
 uploaded, rebinned and filtered once by the same kernels, so the volume must equal the unbounded
 device-resident run's bit for bit -- from a host fan, a device fan, and from the raw file through
-the reader and writer threads (lct_recon_run_file) -- while the device footprint stays below the
-unbounded recon's.  A short or missing file is an LCT_ERR_IO, not a partial volume."""
+the reader and writer threads (lct_recon_run_file), into pinned, pageable and device volumes --
+while the device footprint stays below the unbounded recon's.  A short or missing file is an LCT_ERR_IO, not a partial volume."""
 import numpy as np
 import pytest
 
@@ -56,6 +56,21 @@ def test_bounded_runs_are_bit_identical(scan6, opts):
     h_img.fill_(float("nan"))
     b.run(h_fan, h_img)
     np.testing.assert_array_equal(h_img.numpy(), ref)
+    # pageable volume: slabs copied out of the pinned slots by the writer threads
+    p_img = np.full(b.image_shape, np.nan, dtype=np.float32)
+    b.run(h_fan, p_img)
+    np.testing.assert_array_equal(p_img, ref)
+
+
+def test_unbounded_streamed_run_into_pageable_volume(scan6):
+    """A host fan streams; a pageable volume is downloaded once after the pipeline."""
+    p, fan = scan6["plan"], scan6["fan"]
+    opts = OPTS[0]
+    r = Reconstruction(p, mode=capi.MODE_SCAN, **opts)
+    ref = r.run(fan).cpu().numpy()
+    p_img = np.full(r.image_shape, np.nan, dtype=np.float32)
+    r.run(fan.cpu().pin_memory(), p_img)
+    np.testing.assert_array_equal(p_img, ref)
 
 
 @pytest.mark.parametrize("bounded", [True, False])
@@ -73,6 +88,10 @@ def test_run_file_reads_and_writes_the_reference_files(scan6, tmp_path, bounded)
     r.run_file(tmp_path / "data" / "proj.raw", image_path=out, image=img)
     np.testing.assert_array_equal(img, ref)
     np.testing.assert_array_equal(np.fromfile(out, dtype=np.float32).reshape(ref.shape), ref)
+    # pageable volume only (the writer threads copy it, no file)
+    img.fill(np.nan)
+    r.run_file(tmp_path / "data" / "proj.raw", image=img)
+    np.testing.assert_array_equal(img, ref)
     # file only, twice (the pinned staging is reused)
     out2 = tmp_path / "out" / "volume2.raw"
     for _ in range(2):
