@@ -325,8 +325,9 @@ int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
    one of the two.  A file, or a pageable buffer, is written from pinned slabs by two writer
    threads (both outputs from one download per slab); a pinned buffer alone is downloaded into
    directly.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
-   correction.  The first call allocates the recon's pinned staging (eight fan chunks, three
-   slabs), kept until lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
+   correction.  The recon's pinned staging (eight fan chunks, three slabs) is pinned slot by slot
+   by the reader and writer threads on first use, overlapped with the run, and kept until
+   lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
 int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,
                        lct_stream stream);
 /* Backprojection autotuner (no reference counterpart): times the kernel's slices-per-thread x

@@ -51,6 +51,7 @@ constexpr int kImgRing = 4;               // slabs in the volume ring (host / fi
 constexpr int kFanStage = 8;              // pinned fan chunks of lct_recon_run_file
 constexpr long long kFanChunkBytes = 16LL << 20;  // a chunk: whole views, at most 16 MiB (>= 1 view)
 constexpr int kFanReaders = 4;            // reader threads (chunk c on thread c mod 4)
+static_assert(kFanStage % kFanReaders == 0, "slot s must belong to reader s mod kFanReaders");
 constexpr int kImgStage = 3;              // pinned slabs of the slab writer
 constexpr int kSinkThreads = 2;           // slab writer threads (file writes, pageable copies)
 
@@ -68,9 +69,12 @@ static void rebin_reach(const lct_geom& g, long long& lo, long long& hi) {
 // ----------------------------------------------------------------------------------------------
 class FanReader {
  public:
-  // views [0, nviews) of the run lie at byte0 + v * view_bytes of the file
+  // views [0, nviews) of the run lie at byte0 + v * view_bytes of the file; slots: one pinned
+  // buffer of `chunk` views per slot (null ones are pinned by their reader thread before its
+  // first read into them; slot s is filled only by thread s mod kFanReaders); device: the
+  // caller's CUDA device
   int start(const char* path, long long byte0, long long view_bytes, long long nviews,
-            long long chunk, float* stage, int slots) {
+            long long chunk, std::vector<float*>* slots, int device) {
     fd_ = ::open(path, O_RDONLY);
     if (fd_ < 0) return LCT_ERR_IO;
     struct stat sb;
@@ -83,13 +87,14 @@ class FanReader {
     view_bytes_ = view_bytes;
     nviews_ = nviews;
     chunk_ = chunk;
-    stage_ = stage;
-    slots_ = slots;
-    state_.assign(slots, kFree);
-    held_.resize(slots);
-    for (int i = 0; i < slots; ++i) held_[i] = i - slots;  // "chunk i - slots" done: free for chunk i
-    rel_.resize(slots);
-    for (int i = 0; i < slots; ++i) rel_[i] = {this, i};
+    stage_ = slots;
+    slots_ = (int)slots->size();
+    device_ = device;
+    state_.assign(slots_, kFree);
+    held_.resize(slots_);
+    for (int i = 0; i < slots_; ++i) held_[i] = i - slots_;  // "chunk i - slots" done: free for chunk i
+    rel_.resize(slots_);
+    for (int i = 0; i < slots_; ++i) rel_[i] = {this, i};
     for (int t = 0; t < kFanReaders; ++t) th_.emplace_back([this, t] { loop(t); });
     return LCT_OK;
   }
@@ -101,7 +106,7 @@ class FanReader {
     std::unique_lock<std::mutex> lk(mu_);
     cv_.wait(lk, [&] { return err_ || (state_[slot] == kReady && held_[slot] == c); });
     if (err_) return err_;
-    *data = stage_ + (long long)slot * chunk_ * (view_bytes_ / (long long)sizeof(float));
+    *data = (*stage_)[slot];  // written by its reader before the slot was marked ready
     *nv = std::min(chunk_, nviews_ - c * chunk_);
     return LCT_OK;
   }
@@ -146,6 +151,10 @@ class FanReader {
   // reader thread t: chunks t, t + kFanReaders, ...; chunk c waits for its slot (c mod slots)
   // to be free, i.e. for chunk c - slots to be uploaded
   void loop(int t) {
+    if (cudaSetDevice(device_) != cudaSuccess) {
+      fail(LCT_ERR_CUDA);
+      return;
+    }
     for (long long c = t; c < chunks(); c += kFanReaders) {
       const int slot = (int)(c % slots_);
       {
@@ -156,8 +165,15 @@ class FanReader {
         if (stop_ || err_) return;
         state_[slot] = kReading;
       }
+      float*& buf = (*stage_)[slot];  // this thread's slot: no other thread writes it
+      if (!buf && cudaHostAlloc((void**)&buf, (size_t)(chunk_ * view_bytes_), cudaHostAllocDefault) !=
+                      cudaSuccess) {
+        buf = nullptr;
+        fail(LCT_ERR_ALLOC);
+        return;
+      }
       const long long nv = std::min(chunk_, nviews_ - c * chunk_);
-      char* dst = reinterpret_cast<char*>(stage_) + (long long)slot * chunk_ * view_bytes_;
+      char* dst = reinterpret_cast<char*>(buf);
       long long left = nv * view_bytes_, off = byte0_ + c * chunk_ * view_bytes_;
       int e = LCT_OK;
       while (left > 0) {
@@ -181,10 +197,17 @@ class FanReader {
       if (e) return;
     }
   }
+  void fail(int e) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (!err_) err_ = e;
+    }
+    cv_.notify_all();
+  }
   int fd_ = -1;
   long long byte0_ = 0, view_bytes_ = 0, nviews_ = 0, chunk_ = 1;
-  float* stage_ = nullptr;
-  int slots_ = 0;
+  std::vector<float*>* stage_ = nullptr;
+  int slots_ = 0, device_ = 0;
   std::vector<int> state_;
   std::vector<long long> held_;
   std::vector<Rel> rel_;
@@ -204,8 +227,10 @@ class SlabWriter {
   // path (or null): the volume file, sized and written slab by slab; host (or null): a pageable
   // host volume the slabs are copied into (a download straight into pageable memory would hold
   // the issuing thread until the slab is backprojected, stalling the whole pipeline)
-  int start(const char* path, float* host, long long slab_bytes, int nslabs, float* stage,
-            int slots) {
+  // slots: one pinned buffer of a slab per slot; null ones are pinned in order by the first
+  // writer thread while the first slabs are computed.  device: the caller's CUDA device.
+  int start(const char* path, float* host, long long slab_bytes, int nslabs,
+            std::vector<float*>* slots, int device) {
     if (path) {
       fd_ = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
       if (fd_ < 0) return LCT_ERR_IO;
@@ -217,23 +242,26 @@ class SlabWriter {
     }
     host_ = reinterpret_cast<char*>(host);
     slab_bytes_ = slab_bytes;
-    stage_ = stage;
-    slots_ = slots;
-    busy_.assign(slots, 0);
-    dest_.assign(slots, -1);
-    sub_.resize(slots);
-    for (int i = 0; i < slots; ++i) sub_[i] = {this, i};
-    for (int t = 0; t < kSinkThreads; ++t) th_.emplace_back([this] { loop(); });
+    stage_ = slots;
+    slots_ = (int)slots->size();
+    device_ = device;
+    busy_.assign(slots_, 0);
+    dest_.assign(slots_, -1);
+    have_.assign(slots_, 0);
+    for (int i = 0; i < slots_; ++i) have_[i] = (*slots)[i] != nullptr;
+    sub_.resize(slots_);
+    for (int i = 0; i < slots_; ++i) sub_[i] = {this, i};
+    for (int t = 0; t < kSinkThreads; ++t) th_.emplace_back([this, t] { loop(t); });
     return LCT_OK;
   }
   // pinned slot for the k-th slab written (blocks while its previous slab is being written)
   int slot_for(int k, float** p) {
     const int slot = k % slots_;
     std::unique_lock<std::mutex> lk(mu_);
-    cv_.wait(lk, [&] { return err_ || !busy_[slot]; });
+    cv_.wait(lk, [&] { return err_ || (have_[slot] && !busy_[slot]); });
     if (err_) return err_;
     busy_[slot] = 1;
-    *p = stage_ + (long long)slot * (slab_bytes_ / (long long)sizeof(float));
+    *p = (*stage_)[slot];
     return LCT_OK;
   }
   // once the work queued on s (the slab's download into slot k % slots) is done, write it as
@@ -279,7 +307,25 @@ class SlabWriter {
     }
     s->self->cv_.notify_all();
   }
-  void loop() {
+  void loop(int t) {
+    if (cudaSetDevice(device_) != cudaSuccess) return fail(LCT_ERR_CUDA);
+    if (t == 0) {
+      for (int i = 0; i < slots_; ++i) {
+        float* b = nullptr;
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          if (have_[i]) continue;
+        }
+        if (cudaHostAlloc((void**)&b, (size_t)slab_bytes_, cudaHostAllocDefault) != cudaSuccess)
+          return fail(LCT_ERR_ALLOC);
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          (*stage_)[i] = b;
+          have_[i] = 1;
+        }
+        cv_.notify_all();
+      }
+    }
     for (;;) {
       int slot;
       {
@@ -289,8 +335,13 @@ class SlabWriter {
         slot = ready_.front();
         ready_.erase(ready_.begin());
       }
-      const char* src = reinterpret_cast<const char*>(stage_) + (long long)slot * slab_bytes_;
-      const long long off0 = (long long)dest_[slot] * slab_bytes_;
+      const char* src;
+      long long off0;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        src = reinterpret_cast<const char*>((*stage_)[slot]);
+        off0 = (long long)dest_[slot] * slab_bytes_;
+      }
       if (host_) std::memcpy(host_ + off0, src, (size_t)slab_bytes_);
       long long left = fd_ >= 0 ? slab_bytes_ : 0, off = off0;
       int e = LCT_OK;
@@ -313,12 +364,19 @@ class SlabWriter {
       cv_.notify_all();
     }
   }
+  void fail(int e) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (!err_) err_ = e;
+    }
+    cv_.notify_all();
+  }
   int fd_ = -1;
   char* host_ = nullptr;
   long long slab_bytes_ = 0;
-  float* stage_ = nullptr;
-  int slots_ = 0;
-  std::vector<int> busy_, dest_, ready_;
+  std::vector<float*>* stage_ = nullptr;
+  int slots_ = 0, device_ = 0;
+  std::vector<int> busy_, dest_, ready_, have_;
   std::vector<Sub> sub_;
   std::vector<std::thread> th_;
   std::mutex mu_;
@@ -559,14 +617,10 @@ bool host_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
-// the slab writer's pinned slots, allocated on first use and kept with the recon
-static int ensure_img_stage(lct_recon* r, long long slab) {
-  if (r->h_img_stage) return LCT_OK;
-  int st = cuda_status(cudaHostAlloc((void**)&r->h_img_stage, sizeof(float) * kImgStage * slab,
-                                     cudaHostAllocDefault));
-  if (st) return recon_alloc_status(st);
-  r->img_stage_slots = kImgStage;
-  return LCT_OK;
+// the slab writer's pinned slots (pinned by the writer on first use, kept with the recon)
+static std::vector<float*>* img_slots(lct_recon* r) {
+  if (r->h_img_slots.empty()) r->h_img_slots.assign(kImgStage, nullptr);
+  return &r->h_img_slots;
 }
 
 int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, float* image,
@@ -585,11 +639,11 @@ int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, fl
     // pageable volume: slabs go through the pinned slots and are copied on the writer's threads
     const lct_img& ig = r->info.ig;
     const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
-    int st = ensure_img_stage(r, slab);
+    int dev = 0, st = cuda_status(cudaGetDevice(&dev));
     if (st) return st;
     SlabWriter writer;
     if ((st = writer.start(nullptr, image, (long long)sizeof(float) * slab, r->info.n_blocks_run,
-                           r->h_img_stage, r->img_stage_slots)))
+                           img_slots(r), dev)))
       return st;
     sink.writer = &writer;
     st = run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
@@ -600,9 +654,12 @@ int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, fl
 }
 
 void recon_free_bounded(lct_recon* r) {
-  if (r->h_fan_stage) cudaFreeHost(r->h_fan_stage);
-  if (r->h_img_stage) cudaFreeHost(r->h_img_stage);
-  r->h_fan_stage = r->h_img_stage = nullptr;
+  for (float* p : r->h_fan_slots)
+    if (p) cudaFreeHost(p);
+  for (float* p : r->h_img_slots)
+    if (p) cudaFreeHost(p);
+  r->h_fan_slots.clear();
+  r->h_img_slots.clear();
 }
 
 }  // namespace lct
@@ -695,31 +752,30 @@ LCT_API int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* i
   const long long P = r->piece > 0 ? r->piece : kDefaultPiece;
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
   int st;
-  // pinned staging, allocated on the first call and kept with the recon: chunks of whole views
-  // (pinning costs time in proportion to the bytes, so the chunks are small and many)
+  // pinned staging, kept with the recon: chunks of whole views (pinning costs time in
+  // proportion to the bytes, so the chunks are small and many, and each is pinned by its reader
+  // thread just before its first read)
   const long long view_bytes = (long long)sizeof(float) * r->plane;
   const long long chunk = std::max<long long>(1, std::min<long long>(P, kFanChunkBytes / view_bytes));
-  if (!r->h_fan_stage) {
-    if ((st = cuda_status(cudaHostAlloc((void**)&r->h_fan_stage,
-                                        sizeof(float) * kFanStage * chunk * r->plane,
-                                        cudaHostAllocDefault))))
-      return recon_alloc_status(st);
-    r->fan_stage_slots = kFanStage;
+  if (r->h_fan_slots.empty()) {
+    r->h_fan_slots.assign(kFanStage, nullptr);
+    r->fan_chunk_views = chunk;
   }
+  if (r->fan_chunk_views != chunk) return LCT_ERR_ARG;  // cannot happen: fixed per recon
+  int dev = 0;
+  if ((st = cuda_status(cudaGetDevice(&dev)))) return st;
   // a file, or a pageable volume, is written from pinned slots by the writer's threads (both at
   // once when both are asked for); a pinned volume is downloaded into directly
   const bool use_writer = image_path || !host_pinned(image);
-  if (use_writer && (st = ensure_img_stage(r, slab))) return st;
   FanReader reader;
   SlabWriter writer;
   // file view v of the run's fan views lies at (fan_first + DataOffset + v) views into the file
   // (Src/DataReader.cpp:14, in 64 bits)
   const long long byte0 = (r->fan_first + r->info.data_offset) * view_bytes;
-  if ((st = reader.start(fan_path, byte0, view_bytes, r->fan_count, chunk, r->h_fan_stage,
-                         r->fan_stage_slots)))
+  if ((st = reader.start(fan_path, byte0, view_bytes, r->fan_count, chunk, &r->h_fan_slots, dev)))
     return st;
   if (use_writer && (st = writer.start(image_path, image, (long long)sizeof(float) * slab, nb,
-                                       r->h_img_stage, r->img_stage_slots))) {
+                                       img_slots(r), dev))) {
     reader.finish();
     return st;
   }

@@ -60,10 +60,12 @@ struct lct_recon {
   long long quad_ring = 0;   // views in d_quad (0: g_count, linear)
   int img_ring = 0;          // slabs in d_img for host / file output (0: the whole volume)
   long long device_bytes = 0;
-  // pinned host staging of lct_recon_run_file (allocated on its first call, kept until destroy)
-  float* h_fan_stage = nullptr;
-  float* h_img_stage = nullptr;
-  int fan_stage_slots = 0, img_stage_slots = 0;
+  // pinned host staging of lct_recon_run_file and of pageable host volumes, one buffer per slot:
+  // each is pinned on first use by the reader or writer thread that fills or drains it (so the
+  // pipeline starts after one slot, not after all of them) and kept until destroy
+  std::vector<float*> h_fan_slots;  // fan chunks of fan_chunk_views views
+  long long fan_chunk_views = 0;
+  std::vector<float*> h_img_slots;  // slabs
 };
 
 namespace lct {
