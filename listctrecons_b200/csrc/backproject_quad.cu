@@ -166,18 +166,6 @@ __device__ __forceinline__ float quad_sample_exact(unsigned long long col, unsig
   return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
 }
 
-// The same with the row clamp chosen at run time (warp-uniform): views at a chunk's window edges
-__device__ __forceinline__ float quad_sample_exact_rt(unsigned long long col, unsigned qrow_bytes,
-                                                      int nt, float a, float u, bool clamp) {
-  const float t = __fadd_rd(u, kMagic);
-  const float b = u - (t - kMagic);
-  int rb = __float_as_int(t);
-  if (clamp) rb = min(max(rb, kMagicBits), kMagicBits + nt + 2);
-  const float4 v = __ldg(reinterpret_cast<const float4*>(
-      col + (unsigned long long)(unsigned)rb * qrow_bytes));  // T00, dx, dy, dxy
-  return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
-}
-
 // EXACT column: weight a and 16 * (clamped column bit pattern) added to the biased view base
 __device__ __forceinline__ unsigned long long quad_col_exact(unsigned long long vbias, float p,
                                                              int ns, float& a) {
@@ -412,11 +400,11 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
         const unsigned long long q1 = quad_col_exact(qv.x, fmaf(theta, A.dso_over_ds, A.ws), A.ns, a1);
         const unsigned long long q2 = quad_col_exact(qv.y, fmaf(-theta, A.dso_over_ds, A.ws), A.ns, a2);
         // INSIDE: both samples of every slice lie within the detector rows (no tests, no selects)
-        // the pair weights sum to one in every case -- (-qh2, qh1) / (qh1 - qh2), (0, 1),
-        // (1, 0), (1/2, 1/2) -- so w1 s1 + w2 s2 = s2 + w1 (s1 - s2)
         auto slice_x = [&](int j, auto inside) {
           const float fj = (float)j;
           const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
+          // the pair weights sum to one in every case -- (-qh2, qh1) / (qh1 - qh2), (0, 1),
+          // (1, 0), (1/2, 1/2) -- so w1 s1 + w2 s2 = s2 + w1 (s1 - s2)
           const float in1 = -qh2 * __fdividef(1.0f, qh1 - qh2);
           float w1 = in1;
           if constexpr (!decltype(inside)::value) {
@@ -429,43 +417,24 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
           acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
         };
         // qhat(j) = fmaf(j, kd, h) is monotone in j (monotone rounding of a linear function),
-        // so the view's first and last active slices bound every |qhat| between them: when both
-        // are inside for both views in every lane of the warp, every out test of those slices is
-        // false and the selects are skipped with no change to any result.  The row coordinate
-        // u = qhat + wt + 2 (equal to within a few ulps, far below half a row) then lies in
-        // (1.5, 2 wt + 2.5), inside the quad rows when rows_inside_ok.  Plain comparisons: a NaN
-        // fails them.  Views at the chunk's window edges (a part of the slices active, about a
-        // third of a slab's views) take this path as well as the full ones.
+        // so the chunk's first and last slices bound every |qhat|: when both are inside for both
+        // views in every lane of the warp, every out test of the chunk is false and the selects
+        // are skipped with no change to any result.  The row coordinate u = qhat + wt + 2 (equal
+        // to within a few ulps, far below half a row) then lies in (1.5, 2 wt + 2.5), inside the
+        // quad rows when rows_inside_ok.  Plain comparisons: a NaN fails them.
         bool inside = false;
-        if (jhi > jlo) {
-          const float b1 = fmaf((float)jlo, kd1, h1), b2 = fmaf((float)jlo, kd2, h2);
-          const float e1 = fmaf((float)(jhi - 1), kd1, h1), e2 = fmaf((float)(jhi - 1), kd2, h2);
-          inside = A.rows_inside_ok && fabsf(b1) <= wt && fabsf(e1) <= wt &&
-                   fabsf(b2) <= wt && fabsf(e2) <= wt;
+        if (jlo == 0 && jhi == NZ) {
+          const float e1 = fmaf((float)(NZ - 1), kd1, h1), e2 = fmaf((float)(NZ - 1), kd2, h2);
+          inside = A.rows_inside_ok && fabsf(h1) <= wt && fabsf(e1) <= wt &&
+                   fabsf(h2) <= wt && fabsf(e2) <= wt;
         }
-        const bool all_inside = __all_sync(0xffffffffu, inside);
-        if (all_inside && jlo == 0 && jhi == NZ) {
+        if (__all_sync(0xffffffffu, inside)) {
 #pragma unroll
           for (int j = 0; j < NZ; ++j) slice_x(j, std::true_type{});
         } else {
-          // a part of the slices, or samples that may leave the rows: one predicated loop whose
-          // tests, selects and row clamps run only when some lane needs them (all_inside is
-          // warp-uniform)
 #pragma unroll
-          for (int j = 0; j < NZ; ++j) {
-            if (j < jlo || j >= jhi) continue;
-            const float fj = (float)j;
-            const float qh1 = fmaf(fj, kd1, h1), qh2 = fmaf(fj, kd2, h2);
-            const float in1 = -qh2 * __fdividef(1.0f, qh1 - qh2);
-            float w1 = in1;
-            if (!all_inside) {
-              const bool out1 = fabsf(qh1) > wt, out2 = fabsf(qh2) > wt;
-              w1 = out1 ? (out2 ? 0.5f : 0.0f) : (out2 ? 1.0f : in1);
-            }
-            const float s1 = quad_sample_exact_rt(q1, A.qrow_bytes, A.nt, a1, fmaf(fj, kd1, u1), !all_inside);
-            const float s2 = quad_sample_exact_rt(q2, A.qrow_bytes, A.nt, a2, fmaf(fj, kd2, u2), !all_inside);
-            acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
-          }
+          for (int j = 0; j < NZ; ++j)
+            if (j >= jlo && j < jhi) slice_x(j, std::false_type{});
         }
         continue;
       }
