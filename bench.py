@@ -383,11 +383,13 @@ def plain_gpu(w, geo, ph, ours_value):
             secs = rec["reconstruct_seconds"] * w["blocks"] / rec["n_blocks"]
             runs[name] = {"value": upd / secs / 1e9, "unit": UNIT, "s_per_volume": secs,
                           "blocks_timed": rec["n_blocks"]}
-            m = re.search(r"\[B200\] create ([0-9.]+) s, run ([0-9.]+) s, destroy ([0-9.]+) s",
-                          r.stdout)
+            m = re.search(r"\[B200\] create ([0-9.]+) s, run ([0-9.]+) s, destroy ([0-9.]+) s; "
+                          r"reads ([0-9.]+) s .*waits for reads ([0-9.]+) s, for the writer "
+                          r"([0-9.]+) s", r.stdout)
             if m:  # the whole-scan type's split of reconstruct() (all blocks timed, unscaled)
-                runs[name]["split_s"] = dict(zip(("create", "run", "destroy"),
-                                                 map(float, m.groups())))
+                runs[name]["split_s"] = dict(zip(
+                    ("create", "run", "destroy", "reads_thread_s", "wait_reads", "wait_writer"),
+                    map(float, m.groups())))
     out = runs.pop("reference")
     if "value" in out:
         out["speedup_e2e"] = ours_value / out["value"]

@@ -330,6 +330,10 @@ int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
    lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
 int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,
                        lct_stream stream);
+/* File I/O of the last lct_recon_run_file, seconds: s3[0] = time the reader threads spent in
+   reads (summed over threads), s3[1] = time the pipeline waited for fan chunks not yet read,
+   s3[2] = time it waited for a free slab slot of the writer.  Zeros before the first call. */
+int lct_recon_io_times(const lct_recon* r, float* s3);
 /* Backprojection autotuner (no reference counterpart): times the kernel's slices-per-thread x
    CTAs-per-SM variants on this recon's buffers, keeps the fastest in the recon, and caches it per
    geometry class for the process.  Synchronous; returns the choice. */

@@ -155,6 +155,7 @@ SIGNATURES: dict[str, tuple] = {
     "lct_recon_run_file": (I32, [P, C.c_char_p, C.c_char_p, P, P]),
     "lct_recon_run": (I32, [P, P, I64, I32, P, I32, P]),
     "lct_recon_last_times": (I32, [P, P]),
+    "lct_recon_io_times": (I32, [P, P]),
     "lct_recon_fan_range": (I32, [P, C.POINTER(I64), C.POINTER(I64)]),
     "lct_recon_stats_get": (I32, [P, C.POINTER(ReconStats)]),
     "lct_recon_destroy": (None, [P]),

@@ -27,7 +27,9 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cerrno>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <condition_variable>
@@ -45,6 +47,10 @@ const float* plan_angles(const lct_plan* p);
 #include "recon_internal.h"
 
 namespace lct {
+
+static double wall_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 constexpr long long kDefaultPiece = 512;  // views per rebin / filter / pack step
 constexpr int kImgRing = 4;               // slabs in the volume ring (host / file output)
@@ -100,11 +106,15 @@ class FanReader {
   }
   long long chunks() const { return (nviews_ + chunk_ - 1) / chunk_; }
   long long chunk() const { return chunk_; }
+  double read_seconds() const { return (double)read_ns_.load() * 1e-9; }
+  double wait_seconds() const { return wait_s_; }
   // blocks until chunk c is in its pinned slot
   int acquire(long long c, const float** data, long long* nv) {
     const int slot = (int)(c % slots_);
+    const double t0 = wall_seconds();
     std::unique_lock<std::mutex> lk(mu_);
     cv_.wait(lk, [&] { return err_ || (state_[slot] == kReady && held_[slot] == c); });
+    wait_s_ += wall_seconds() - t0;
     if (err_) return err_;
     *data = (*stage_)[slot];  // written by its reader before the slot was marked ready
     *nv = std::min(chunk_, nviews_ - c * chunk_);
@@ -172,6 +182,7 @@ class FanReader {
         fail(LCT_ERR_ALLOC);
         return;
       }
+      const double t0 = wall_seconds();
       const long long nv = std::min(chunk_, nviews_ - c * chunk_);
       char* dst = reinterpret_cast<char*>(buf);
       long long left = nv * view_bytes_, off = byte0_ + c * chunk_ * view_bytes_;
@@ -187,6 +198,7 @@ class FanReader {
         off += n;
         left -= n;
       }
+      read_ns_ += (long long)((wall_seconds() - t0) * 1e9);
       {
         std::lock_guard<std::mutex> lk(mu_);
         if (e) err_ = e;
@@ -206,6 +218,8 @@ class FanReader {
   }
   int fd_ = -1;
   long long byte0_ = 0, view_bytes_ = 0, nviews_ = 0, chunk_ = 1;
+  std::atomic<long long> read_ns_{0};  // time in reads, summed over the threads
+  double wait_s_ = 0.0;                // the pipeline's waits in acquire (its thread only)
   std::vector<float*>* stage_ = nullptr;
   int slots_ = 0, device_ = 0;
   std::vector<int> state_;
@@ -257,8 +271,10 @@ class SlabWriter {
   // pinned slot for the k-th slab written (blocks while its previous slab is being written)
   int slot_for(int k, float** p) {
     const int slot = k % slots_;
+    const double t0 = wall_seconds();
     std::unique_lock<std::mutex> lk(mu_);
     cv_.wait(lk, [&] { return err_ || (have_[slot] && !busy_[slot]); });
+    wait_s_ += wall_seconds() - t0;
     if (err_) return err_;
     busy_[slot] = 1;
     *p = (*stage_)[slot];
@@ -274,6 +290,7 @@ class SlabWriter {
     }
     return cuda_status(cudaLaunchHostFunc(s, &SlabWriter::on_downloaded, &sub_[slot]));
   }
+  double wait_seconds() const { return wait_s_; }
   int finish() {
     {
       std::unique_lock<std::mutex> lk(mu_);
@@ -371,6 +388,7 @@ class SlabWriter {
     }
     cv_.notify_all();
   }
+  double wait_s_ = 0.0;  // the pipeline's waits for a free slot (its thread only)
   int fd_ = -1;
   char* host_ = nullptr;
   long long slab_bytes_ = 0;
@@ -789,5 +807,14 @@ LCT_API int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* i
   st = run_forked(r, s, [&] { return run_pipeline(r, feed, sink, s, r->ss); });
   const int st_r = reader.finish();
   const int st_w = use_writer ? writer.finish() : LCT_OK;
+  r->io_times[0] = (float)reader.read_seconds();
+  r->io_times[1] = (float)reader.wait_seconds();
+  r->io_times[2] = (float)writer.wait_seconds();
   return st ? st : (st_r ? st_r : st_w);
+}
+
+LCT_API int lct_recon_io_times(const lct_recon* r, float* s3) {
+  if (!r || !s3) return LCT_ERR_ARG;
+  for (int i = 0; i < 3; ++i) s3[i] = r->io_times[i];
+  return LCT_OK;
 }

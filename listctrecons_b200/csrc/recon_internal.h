@@ -40,6 +40,7 @@ struct lct_recon {
   CUtensorMap tma_map;       // d_quad as the staged kernel's tensor
   cudaEvent_t ev[6] = {};
   float times[5] = {};
+  float io_times[3] = {};  // lct_recon_io_times
   lct_cnn* cnn = nullptr;    // learned correction after backprojection (not owned)
   float cnn_bound = 0.f;
   float* d_plain = nullptr;  // plain FDK volume when the learned correction runs

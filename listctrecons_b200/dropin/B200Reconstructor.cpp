@@ -15,7 +15,7 @@
 //
 // Defaults: exact interpolation, the BF16x6 tensor-core filter, border addressing, a bounded
 // device footprint (lct_recon_create_bounded) fed by lct_recon_run_file's reader threads.  The
-// recon's create, run and destroy times are printed on one "[B200]" line.
+// recon's create, run and destroy times and its file I/O times are printed on one "[B200]" line.
 // Environment switches, as for the stage drop-in: LCT_DROPIN_INTERP=tex8|exact,
 // LCT_DROPIN_FILTER=fp32|bf16x3|bf16x6, LCT_DROPIN_ADDR=border|clamp|legacy.  LEGACY (the
 // reference's clamped first block) needs the whole filtered views on the device: that run
@@ -206,14 +206,17 @@ void B200FDKReconstructor::reconstruct(const ReconData* mr) {
     if (fan) cudaFreeHost(fan);
   }
   const clk::time_point t2 = clk::now();
+  float io[3] = {0.f, 0.f, 0.f};
+  if (r) lct_recon_io_times(r, io);
   if (r) lct_recon_destroy(r);
   lct_plan_destroy(plan);
   const clk::time_point t3 = clk::now();
   auto secs = [](clk::time_point a, clk::time_point b) {
     return std::chrono::duration<double>(b - a).count();
   };
-  std::printf("[B200] create %.4f s, run %.4f s, destroy %.4f s\n", secs(t0, t1), secs(t1, t2),
-              secs(t2, t3));
+  std::printf("[B200] create %.4f s, run %.4f s, destroy %.4f s; reads %.4f s (summed over the "
+              "reader threads), waits for reads %.4f s, for the writer %.4f s\n",
+              secs(t0, t1), secs(t1, t2), secs(t2, t3), io[0], io[1], io[2]);
   std::cout << "Reconstruction of " << nb << " blocks finished." << std::endl;
 }
 

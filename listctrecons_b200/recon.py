@@ -196,6 +196,13 @@ class Reconstruction:
         capi.check(self._lib.lct_recon_last_times(self._h, t))
         return dict(zip(["h2d", "rebin", "filter", "backproject", "d2h"], list(t)))
 
+    def io_times(self) -> dict:
+        """lct_recon_io_times: seconds of the last run_file -- reads (summed over the reader
+        threads), pipeline waits for fan chunks, pipeline waits for writer slots."""
+        t = (C.c_float * 3)()
+        capi.check(self._lib.lct_recon_io_times(self._h, t))
+        return dict(zip(["read", "wait_read", "wait_write"], list(t)))
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:

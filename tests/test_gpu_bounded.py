@@ -87,6 +87,8 @@ def test_run_file_reads_and_writes_the_reference_files(scan6, tmp_path, bounded)
     img = np.full(r.image_shape, np.nan, dtype=np.float32)
     r.run_file(tmp_path / "data" / "proj.raw", image_path=out, image=img)
     np.testing.assert_array_equal(img, ref)
+    io = r.io_times()  # the readers read something; waits are never negative
+    assert io["read"] > 0.0 and io["wait_read"] >= 0.0 and io["wait_write"] >= 0.0
     np.testing.assert_array_equal(np.fromfile(out, dtype=np.float32).reshape(ref.shape), ref)
     # pageable volume only (the writer threads copy it, no file)
     img.fill(np.nan)
