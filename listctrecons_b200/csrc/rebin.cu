@@ -185,6 +185,33 @@ __global__ void __launch_bounds__(256) rebin_fan2par_scan4_kernel(
 #pragma unroll
     for (int c = 0; c < 4; ++c) hi[c] = fl[c] != f0;
     const long long v0 = g + f0 - fan_first;
+    float* o = par + lv * plane + is0;
+    // the common case: all kTaps fan views present, none clamped or zero-filled, and consecutive
+    // in the buffer (no ring wrap among them) -- one base pointer and the plane stride address
+    // every tap and no load is predicated (0.44 ms instead of 0.47 ms on config 2's scan)
+    const long long slot0 = fan_ring > 0 ? (v0 >= 0 ? v0 % fan_ring : -1) : v0;
+    if (nk == kRebinViews && v0 >= 0 && v0 + kTaps <= fan_count &&
+        (fan_ring == 0 || slot0 + kTaps <= fan_ring)) {
+      const float4* b = reinterpret_cast<const float4*>(fan + slot0 * plane + is0);
+      const long long p4 = plane >> 2;  // ns is a multiple of 4
+      for (int it = it0; it < it1; ++it) {
+        const long long r4 = ((long long)it * a.ns) >> 2;
+        float4 t[kTaps];
+#pragma unroll
+        for (int m = 0; m < kTaps; ++m) t[m] = __ldg(b + m * p4 + r4);
+#pragma unroll
+        for (int k = 0; k < kRebinViews; ++k) {
+          const float4 lo = t[k], mid = t[k + 1], up = t[k + 2];
+          float4 out;
+          out.x = fmaf(w[0], hi[0] ? up.x : mid.x, (1.0f - w[0]) * (hi[0] ? mid.x : lo.x));
+          out.y = fmaf(w[1], hi[1] ? up.y : mid.y, (1.0f - w[1]) * (hi[1] ? mid.y : lo.y));
+          out.z = fmaf(w[2], hi[2] ? up.z : mid.z, (1.0f - w[2]) * (hi[2] ? mid.z : lo.z));
+          out.w = fmaf(w[3], hi[3] ? up.w : mid.w, (1.0f - w[3]) * (hi[3] ? mid.w : lo.w));
+          *reinterpret_cast<float4*>(o + k * plane + (long long)it * a.ns) = out;
+        }
+      }
+      continue;
+    }
     const float4* p[kTaps];
     bool ok[kTaps];
 #pragma unroll
@@ -199,7 +226,6 @@ __global__ void __launch_bounds__(256) rebin_fan2par_scan4_kernel(
       if (fan_ring > 0) v %= fan_ring;
       p[m] = reinterpret_cast<const float4*>(fan + v * plane + is0);
     }
-    float* o = par + lv * plane + is0;
     for (int it = it0; it < it1; ++it) {
       const long long r4 = ((long long)it * a.ns) >> 2;  // float4 offset of the row segment
       float4 t[kTaps];
