@@ -23,6 +23,7 @@
 // volume through slab writer threads (64-bit offsets) -- RawDataReader::readData and RawImageWriter
 // (Src/ImageWriter.cpp:9-43) for whole scans.
 #include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -47,6 +48,45 @@ const float* plan_angles(const lct_plan* p);
 #include "recon_internal.h"
 
 namespace lct {
+
+int pinned_alloc(size_t bytes, PinnedBuf& b) {
+  constexpr size_t kHuge = 2u << 20;
+  const size_t len = (bytes + kHuge - 1) / kHuge * kHuge;
+  void* m = ::mmap(nullptr, len + kHuge, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+  if (m != MAP_FAILED) {
+    char* p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(m) + kHuge - 1) & ~(uintptr_t)(kHuge - 1));
+    ::madvise(p, len, MADV_HUGEPAGE);  // a request: 4 KiB pages if refused
+    for (size_t o = 0; o < len; o += kHuge) p[o] = 0;
+    if (cudaHostRegister(p, len, cudaHostRegisterDefault) == cudaSuccess) {
+      b.p = reinterpret_cast<float*>(p);
+      b.map = m;
+      b.map_bytes = len + kHuge;
+      return LCT_OK;
+    }
+    cudaGetLastError();
+    ::munmap(m, len + kHuge);
+  }
+  void* h = nullptr;
+  if (cudaHostAlloc(&h, bytes, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return LCT_ERR_ALLOC;
+  }
+  b.p = static_cast<float*>(h);
+  b.map = nullptr;
+  b.map_bytes = 0;
+  return LCT_OK;
+}
+
+void pinned_free(PinnedBuf& b) {
+  if (!b.p) return;
+  if (b.map) {
+    cudaHostUnregister(b.p);
+    ::munmap(b.map, b.map_bytes);
+  } else {
+    cudaFreeHost(b.p);
+  }
+  b = PinnedBuf{};
+}
 
 static double wall_seconds() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -80,7 +120,7 @@ class FanReader {
   // first read into them; slot s is filled only by thread s mod kFanReaders); device: the
   // caller's CUDA device
   int start(const char* path, long long byte0, long long view_bytes, long long nviews,
-            long long chunk, std::vector<float*>* slots, int device) {
+            long long chunk, std::vector<PinnedBuf>* slots, int device) {
     fd_ = ::open(path, O_RDONLY);
     if (fd_ < 0) return LCT_ERR_IO;
     struct stat sb;
@@ -116,7 +156,7 @@ class FanReader {
     cv_.wait(lk, [&] { return err_ || (state_[slot] == kReady && held_[slot] == c); });
     wait_s_ += wall_seconds() - t0;
     if (err_) return err_;
-    *data = (*stage_)[slot];  // written by its reader before the slot was marked ready
+    *data = (*stage_)[slot].p;  // written by its reader before the slot was marked ready
     *nv = std::min(chunk_, nviews_ - c * chunk_);
     return LCT_OK;
   }
@@ -175,16 +215,14 @@ class FanReader {
         if (stop_ || err_) return;
         state_[slot] = kReading;
       }
-      float*& buf = (*stage_)[slot];  // this thread's slot: no other thread writes it
-      if (!buf && cudaHostAlloc((void**)&buf, (size_t)(chunk_ * view_bytes_), cudaHostAllocDefault) !=
-                      cudaSuccess) {
-        buf = nullptr;
+      PinnedBuf& buf = (*stage_)[slot];  // this thread's slot: no other thread writes it
+      if (!buf.p && pinned_alloc((size_t)(chunk_ * view_bytes_), buf) != LCT_OK) {
         fail(LCT_ERR_ALLOC);
         return;
       }
       const double t0 = wall_seconds();
       const long long nv = std::min(chunk_, nviews_ - c * chunk_);
-      char* dst = reinterpret_cast<char*>(buf);
+      char* dst = reinterpret_cast<char*>(buf.p);
       long long left = nv * view_bytes_, off = byte0_ + c * chunk_ * view_bytes_;
       int e = LCT_OK;
       while (left > 0) {
@@ -220,7 +258,7 @@ class FanReader {
   long long byte0_ = 0, view_bytes_ = 0, nviews_ = 0, chunk_ = 1;
   std::atomic<long long> read_ns_{0};  // time in reads, summed over the threads
   double wait_s_ = 0.0;                // the pipeline's waits in acquire (its thread only)
-  std::vector<float*>* stage_ = nullptr;
+  std::vector<PinnedBuf>* stage_ = nullptr;
   int slots_ = 0, device_ = 0;
   std::vector<int> state_;
   std::vector<long long> held_;
@@ -244,7 +282,7 @@ class SlabWriter {
   // slots: one pinned buffer of a slab per slot; null ones are pinned in order by the first
   // writer thread while the first slabs are computed.  device: the caller's CUDA device.
   int start(const char* path, float* host, long long slab_bytes, int nslabs,
-            std::vector<float*>* slots, int device) {
+            std::vector<PinnedBuf>* slots, int device) {
     if (path) {
       fd_ = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
       if (fd_ < 0) return LCT_ERR_IO;
@@ -262,7 +300,7 @@ class SlabWriter {
     busy_.assign(slots_, 0);
     dest_.assign(slots_, -1);
     have_.assign(slots_, 0);
-    for (int i = 0; i < slots_; ++i) have_[i] = (*slots)[i] != nullptr;
+    for (int i = 0; i < slots_; ++i) have_[i] = (*slots)[i].p != nullptr;
     sub_.resize(slots_);
     for (int i = 0; i < slots_; ++i) sub_[i] = {this, i};
     for (int t = 0; t < kSinkThreads; ++t) th_.emplace_back([this, t] { loop(t); });
@@ -277,7 +315,7 @@ class SlabWriter {
     wait_s_ += wall_seconds() - t0;
     if (err_) return err_;
     busy_[slot] = 1;
-    *p = (*stage_)[slot];
+    *p = (*stage_)[slot].p;
     return LCT_OK;
   }
   // once the work queued on s (the slab's download into slot k % slots) is done, write it as
@@ -328,13 +366,12 @@ class SlabWriter {
     if (cudaSetDevice(device_) != cudaSuccess) return fail(LCT_ERR_CUDA);
     if (t == 0) {
       for (int i = 0; i < slots_; ++i) {
-        float* b = nullptr;
+        PinnedBuf b;
         {
           std::lock_guard<std::mutex> lk(mu_);
           if (have_[i]) continue;
         }
-        if (cudaHostAlloc((void**)&b, (size_t)slab_bytes_, cudaHostAllocDefault) != cudaSuccess)
-          return fail(LCT_ERR_ALLOC);
+        if (pinned_alloc((size_t)slab_bytes_, b) != LCT_OK) return fail(LCT_ERR_ALLOC);
         {
           std::lock_guard<std::mutex> lk(mu_);
           (*stage_)[i] = b;
@@ -356,7 +393,7 @@ class SlabWriter {
       long long off0;
       {
         std::lock_guard<std::mutex> lk(mu_);
-        src = reinterpret_cast<const char*>((*stage_)[slot]);
+        src = reinterpret_cast<const char*>((*stage_)[slot].p);
         off0 = (long long)dest_[slot] * slab_bytes_;
       }
       if (host_) std::memcpy(host_ + off0, src, (size_t)slab_bytes_);
@@ -392,7 +429,7 @@ class SlabWriter {
   int fd_ = -1;
   char* host_ = nullptr;
   long long slab_bytes_ = 0;
-  std::vector<float*>* stage_ = nullptr;
+  std::vector<PinnedBuf>* stage_ = nullptr;
   int slots_ = 0, device_ = 0;
   std::vector<int> busy_, dest_, ready_, have_;
   std::vector<Sub> sub_;
@@ -636,8 +673,8 @@ bool host_pinned(const void* p) {
 }
 
 // the slab writer's pinned slots (pinned by the writer on first use, kept with the recon)
-static std::vector<float*>* img_slots(lct_recon* r) {
-  if (r->h_img_slots.empty()) r->h_img_slots.assign(kImgStage, nullptr);
+static std::vector<PinnedBuf>* img_slots(lct_recon* r) {
+  if (r->h_img_slots.empty()) r->h_img_slots.assign(kImgStage, PinnedBuf{});
   return &r->h_img_slots;
 }
 
@@ -672,10 +709,8 @@ int recon_run_bounded_ptr(lct_recon* r, const float* fan, bool fan_on_device, fl
 }
 
 void recon_free_bounded(lct_recon* r) {
-  for (float* p : r->h_fan_slots)
-    if (p) cudaFreeHost(p);
-  for (float* p : r->h_img_slots)
-    if (p) cudaFreeHost(p);
+  for (PinnedBuf& b : r->h_fan_slots) pinned_free(b);
+  for (PinnedBuf& b : r->h_img_slots) pinned_free(b);
   r->h_fan_slots.clear();
   r->h_img_slots.clear();
 }
@@ -776,7 +811,7 @@ LCT_API int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* i
   const long long view_bytes = (long long)sizeof(float) * r->plane;
   const long long chunk = std::max<long long>(1, std::min<long long>(P, kFanChunkBytes / view_bytes));
   if (r->h_fan_slots.empty()) {
-    r->h_fan_slots.assign(kFanStage, nullptr);
+    r->h_fan_slots.assign(kFanStage, PinnedBuf{});
     r->fan_chunk_views = chunk;
   }
   if (r->fan_chunk_views != chunk) return LCT_ERR_ARG;  // cannot happen: fixed per recon
