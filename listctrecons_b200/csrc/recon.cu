@@ -585,7 +585,7 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
   int st;
   // events: 5 for the caller's fork and join, per slab: views ready, backprojected, corrected;
   // per piece: uploaded, packed
-  const long long n_pieces = r->g_count / kStreamPiece + nb + 1;
+  const long long n_pieces = r->g_count / kStreamPiece + nb + 2;  // + the first slab's short piece
   const size_t n_ev = 5 + 3 * (size_t)nb + 2 * (size_t)n_pieces;
   while (r->sev.size() < n_ev) {
     cudaEvent_t e;
@@ -644,7 +644,8 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
     const long long slab_end = std::min(gend[b], r->g_first + r->g_count);
     int bp_lo = 0, parts = 0;
     while (slab_end > done) {
-      const long long target = std::min(slab_end, done + kStreamPiece);
+      long long target = std::min(slab_end, done + kStreamPiece);
+      if (split) target = first_part_target(done, target, gfirst[b], g.n_proj_turn / 2);
       const long long need = std::min(r->fan_count, target - 1 + shift_hi + 1 - r->fan_first);
       if (piece >= n_pieces) return LCT_ERR_ARG;  // cannot happen: pieces are counted above
       if (need > up) {

@@ -478,7 +478,7 @@ static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink
   const long long plane = r->plane;
   const long long P = r->piece > 0 ? r->piece : kDefaultPiece;
   int st;
-  const long long n_pieces = r->g_count / P + nb + 1;
+  const long long n_pieces = r->g_count / P + nb + 2;  // + the first slab's short piece
   cudaEvent_t* ev = nullptr;
   if ((st = run_events(r, n_pieces, &ev))) return st;
   cudaEvent_t* ev_views = ev + 5;
@@ -539,7 +539,8 @@ static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink
     const long long slab_end = std::min(gend[b], r->g_first + r->g_count);
     int bp_lo = 0, parts = 0;
     while (slab_end > done) {
-      const long long target = std::min(slab_end, done + P);
+      long long target = std::min(slab_end, done + P);
+      if (split) target = first_part_target(done, target, gfirst[b], g.n_proj_turn / 2);
       const long long need = std::min(r->fan_count, target + reach_hi + 1 - r->fan_first);
       if (piece >= n_pieces) return LCT_ERR_ARG;  // cannot happen: pieces are counted above
       if (!feed.dev && need > up) {

@@ -17,6 +17,16 @@ void streams_destroy(StreamSet& ss);
 int streams_fork(const StreamSet& ss, cudaStream_t s, cudaEvent_t ev);
 int streams_join(const StreamSet& ss, cudaStream_t s, const cudaEvent_t* ev4);
 
+// The first slab of a streamed run is backprojected in parts as its views arrive; a part needs
+// the conjugates (half a turn on) of its pairs.  The piece that crosses half a turn ends
+// kFirstPairs pairs past it, so the first part starts then and not up to a piece later.
+constexpr long long kFirstPairs = 64;
+inline long long first_part_target(long long done, long long target, long long gfirst,
+                                   long long half) {
+  const long long pivot = gfirst + half + kFirstPairs;
+  return done < pivot && target > pivot ? pivot : target;
+}
+
 // Pinned host staging: a 2 MiB-aligned anonymous mapping with transparent huge pages requested,
 // faulted in one touch per 2 MiB and registered with the driver -- about twice as fast to set up
 // as cudaHostAlloc, which pins 4 KiB pages (measured on B200 hosts: 128 MB in 30 ms against

@@ -247,6 +247,30 @@ void orc_rebin_pi_ori(const orc_geom* g, const float* fan, double* out, int inte
       }
 }
 
+/* The texture coordinates CUDA/Rebiner.cu:156-179 samples at (its FP32 expressions, as the TEXEMU
+   branch above), [n_angle][nt][ns][3] = (x, y, z): the texture unit sampled at these is the
+   hardware reference for the TEX8 PI-original rebin. */
+void orc_rebin_pi_ori_coords(const orc_geom* g, float* xyz) {
+  const long ns = g->ns, nt = g->nt;
+#pragma omp parallel for schedule(static)
+  for (int ia = 0; ia < g->n_angle; ++ia)
+    for (int it = 0; it < g->nt; ++it)
+      for (int is = 0; is < g->ns; ++is) {
+        float s = ((float)is - g->ws) * g->ds;
+        float gamma = asinf(s / g->dso);
+        float pidx = gamma * g->dso / g->ds + g->ws;
+        double num = (double)(((float)it - g->wt) * g->pitch / (float)(2 * (g->nt - 1))) -
+                     (double)(gamma * g->pitch) / (2 * REF_PI);
+        float q = (float)(num / (double)cosf(gamma));
+        float qidx = q / g->dt + g->wt;
+        float bidx = (float)ia + gamma / g->orbit + (float)g->add_projections;
+        float* o = xyz + 3 * (((long)ia * nt + it) * ns + is);
+        o[0] = pidx + 0.5f;
+        o[1] = qidx + 0.5f;
+        o[2] = bidx + 0.5f;
+      }
+}
+
 /* CUDA/PreWeighting.cu:8-29, in place, [n_angle][nt][ns] */
 void orc_weight_pi_ori(const orc_geom* g, double* proj) {
   const long ns = g->ns, nt = g->nt;

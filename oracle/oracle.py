@@ -67,6 +67,7 @@ def lib() -> C.CDLL:
             "orc_rebin_fan2par": (None, [G, P, P, C.c_int, C.c_int]),
             "orc_rebin_null": (None, [G, P, P, C.c_int]),
             "orc_rebin_pi_ori": (None, [G, P, P, C.c_int, C.c_int]),
+            "orc_rebin_pi_ori_coords": (None, [G, P]),
             "orc_weight_pi_ori": (None, [G, P]),
             "orc_ramp_taps": (None, [C.c_int, C.c_float, P]),
             "orc_shepp_logan_taps": (None, [C.c_int, C.c_float, P]),
@@ -150,6 +151,14 @@ def rebin_pi_ori(g, fan, interp=TEXEMU, addr=BORDER):
     fan = _f32(fan)
     out = np.zeros((g.n_angle, g.nt, g.ns), dtype=np.float64)
     lib().orc_rebin_pi_ori(C.byref(geom_from(g)), fan.ctypes.data, out.ctypes.data, interp, addr)
+    return out
+
+
+def rebin_pi_ori_coords(g):
+    """[n_angle][nt][ns][3] float32 texture coordinates the reference's PI-original rebin samples
+    at (CUDA/Rebiner.cu:156-179, its FP32 expressions)."""
+    out = np.zeros((g.n_angle, g.nt, g.ns, 3), dtype=np.float32)
+    lib().orc_rebin_pi_ori_coords(C.byref(geom_from(g)), out.ctypes.data)
     return out
 
 

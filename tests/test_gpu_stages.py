@@ -113,6 +113,33 @@ def test_rebin_null_and_pi_ori(setup):
         assert orc.rel_l2(out.cpu().numpy(), ref) < (1e-6 if interp == capi.INTERP_EXACT else 2e-3)
 
 
+def test_rebin_pi_ori_tex8_is_the_texture_unit_at_the_reference_coordinates(setup):
+    """TEX8 PI-original rebin samples the fan block through the texture unit, as the reference
+    does (CUDA/Rebiner.cu:156-179).  Reference here: the same unit (the probe library's 3-D
+    texture) sampled at the coordinates the oracle computes with the reference's FP32
+    expressions.  The two coordinate computations differ only by FMA contraction and libm ulps,
+    which can move an 8-bit weight by one step for a few samples; the software emulation above
+    is held only to 2e-3 because the unit's z combination is not reproduced exactly."""
+    torch, g, fan = setup["torch"], setup["g"], setup["fan"]
+    lib = capi.lib()
+    d_fan = _dev(torch, fan)
+    out = torch.empty((g.n_angle, g.nt, g.ns), dtype=torch.float32, device="cuda")
+    capi.check(lib.lct_rebin_pi_ori(C.byref(g), d_fan.data_ptr(), out.data_ptr(),
+                                    capi.INTERP_TEX8, capi.ADDR_BORDER, None))
+    _sync(torch)
+    coords = np.ascontiguousarray(orc.rebin_pi_ori_coords(g).reshape(-1, 3))
+    vol = np.ascontiguousarray(fan[: g.n_angle_add], dtype=np.float32)
+    hw = np.zeros(len(coords), dtype=np.float32)
+    rc = capi.load_probe().lctp_tex3d_sample(vol.ctypes.data, g.ns, g.nt, g.n_angle_add,
+                                             coords.ctypes.data, len(coords), 0, hw.ctypes.data)
+    assert rc == 0, f"cudaError {rc}"
+    got = out.cpu().numpy().ravel()
+    err = orc.rel_l2(got, hw)
+    print(f"PI-original TEX8 vs texture unit at the reference's coordinates: rel_l2={err:.3e}, "
+          f"identical samples {np.mean(got == hw):.5f}")
+    assert err < 1e-5
+
+
 def test_weight_pi_ori(setup):
     torch, g, fan = setup["torch"], setup["g"], setup["fan"]
     par = fan[: g.n_angle].copy()
