@@ -200,7 +200,7 @@ LCT_API int lct_batch_create(const lct_plan* const* plans, int n, const lct_reco
 static int batch_run_streamed(lct_batch* b, const float* const* fans, const int64_t* fan_view0,
                               float* const* images, int image_on_device, cudaStream_t s) {
   int st = streams_create(b->ss);
-  while (!st && b->sev.size() < 5) {
+  while (!st && b->sev.size() < (size_t)kForkJoinEvents) {
     cudaEvent_t e;
     st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if (!st) b->sev.push_back(e);

@@ -540,11 +540,17 @@ int streams_create(StreamSet& ss) {
     const int st = cuda_status(cudaStreamCreateWithFlags(a, cudaStreamNonBlocking));
     if (st) return st;
   }
+  if (!ss.prep) {
+    int least = 0, greatest = 0;
+    int st = cuda_status(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    if (!st) st = cuda_status(cudaStreamCreateWithPriority(&ss.prep, cudaStreamNonBlocking, greatest));
+    if (st) return st;
+  }
   return LCT_OK;
 }
 
 void streams_destroy(StreamSet& ss) {
-  for (cudaStream_t* a : {&ss.up, &ss.down, &ss.bp[0], &ss.bp[1], &ss.cnn})
+  for (cudaStream_t* a : {&ss.up, &ss.down, &ss.bp[0], &ss.bp[1], &ss.cnn, &ss.prep})
     if (*a) {
       cudaStreamDestroy(*a);
       *a = nullptr;
@@ -553,17 +559,18 @@ void streams_destroy(StreamSet& ss) {
 
 int streams_fork(const StreamSet& ss, cudaStream_t s, cudaEvent_t ev) {
   int st = cuda_status(cudaEventRecord(ev, s));
-  for (cudaStream_t x : {ss.up, ss.down, ss.bp[0], ss.bp[1], ss.cnn})
+  for (cudaStream_t x : {ss.up, ss.down, ss.bp[0], ss.bp[1], ss.cnn, ss.prep})
     if (!st) st = cuda_status(cudaStreamWaitEvent(x, ev, 0));
   return st;
 }
 
-int streams_join(const StreamSet& ss, cudaStream_t s, const cudaEvent_t* ev4) {
-  const cudaStream_t x[4] = {ss.down, ss.bp[0], ss.bp[1], ss.cnn};  // uploads end in s already
+int streams_join(const StreamSet& ss, cudaStream_t s, const cudaEvent_t* ev5) {
+  // uploads end in prep already
+  const cudaStream_t x[5] = {ss.down, ss.bp[0], ss.bp[1], ss.cnn, ss.prep};
   int st = LCT_OK;
-  for (int i = 0; i < 4 && !st; ++i) {
-    st = cuda_status(cudaEventRecord(ev4[i], x[i]));
-    if (!st) st = cuda_status(cudaStreamWaitEvent(s, ev4[i], 0));
+  for (int i = 0; i < 5 && !st; ++i) {
+    st = cuda_status(cudaEventRecord(ev5[i], x[i]));
+    if (!st) st = cuda_status(cudaStreamWaitEvent(s, ev5[i], 0));
   }
   return st;
 }
@@ -583,16 +590,19 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
   const long long plane = r->plane;
   int st;
-  // events: 5 for the caller's fork and join, per slab: views ready, backprojected, corrected;
+  const cudaStream_t sp = ss.prep;  // per-piece rebin / filter / pack (high priority)
+  (void)s;                          // the caller forks the set from s and joins it back
+  // events: the caller's fork and join, per slab: views ready, backprojected, corrected;
   // per piece: uploaded, packed
-  const long long n_pieces = r->g_count / kStreamPiece + nb + 2;  // + the first slab's short piece
-  const size_t n_ev = 5 + 3 * (size_t)nb + 2 * (size_t)n_pieces;
+  // + the first slab's short pieces (the pivot and at most 64 doublings up to a full piece)
+  const long long n_pieces = r->g_count / kStreamPiece + nb + 2 + 64;
+  const size_t n_ev = kForkJoinEvents + 3 * (size_t)nb + 2 * (size_t)n_pieces;
   while (r->sev.size() < n_ev) {
     cudaEvent_t e;
     if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return st;
     r->sev.push_back(e);
   }
-  cudaEvent_t* ev_views = r->sev.data() + 5;
+  cudaEvent_t* ev_views = r->sev.data() + kForkJoinEvents;
   cudaEvent_t* ev_bp = ev_views + nb;
   cudaEvent_t* ev_cnn = ev_bp + nb;
   cudaEvent_t* ev_up = ev_cnn + nb;
@@ -656,25 +666,25 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
         up = need;
       }
       if ((st = cuda_status(cudaEventRecord(ev_up[piece], ss.up)))) return st;
-      if ((st = cuda_status(cudaStreamWaitEvent(s, ev_up[piece], 0)))) return st;
+      if ((st = cuda_status(cudaStreamWaitEvent(sp, ev_up[piece], 0)))) return st;
       const long long v0 = done - r->g_first, nv = target - done;
       float* par = r->d_par + v0 * plane;
       if ((st = launch_rebin_fan2par_scan(g, r->d_fan, r->fan_first, r->fan_count, par, done, nv,
-                                          r->o.interp, addr0, s)))
+                                          r->o.interp, addr0, sp)))
         return st;
       r->launches++;
       if (r->o.filter_mode != LCT_FILTER_FP32)
-        st = tc_filter(g.ns, par, nv * g.nt, r->d_tc, r->tc_rows, r->o.filter_mode, s);
+        st = tc_filter(g.ns, par, nv * g.nt, r->d_tc, r->tc_rows, r->o.filter_mode, sp);
       else
-        st = launch_filter_rows(g.ns, r->d_h, par, nv * g.nt, LCT_FILTER_FP32, s);
+        st = launch_filter_rows(g.ns, r->d_h, par, nv * g.nt, LCT_FILTER_FP32, sp);
       if (st) return st;
       r->launches += filter_launches(r->o.filter_mode);
       if (r->quads) {
-        if ((st = recon_pack(r, par, nv, v0, packed, s))) return st;
+        if ((st = recon_pack(r, par, nv, v0, packed, sp))) return st;
         r->launches++;
       }
       done = target;
-      if ((st = cuda_status(cudaEventRecord(ev_packed[piece], s)))) return st;
+      if ((st = cuda_status(cudaEventRecord(ev_packed[piece], sp)))) return st;
       ++piece;
       // a pair starting at local view ia also reads its conjugate ia + half: a part takes the
       // pair starts whose conjugates are packed too
@@ -688,7 +698,7 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
       }
     }
     // every view of the slab's window is packed
-    if ((st = cuda_status(cudaEventRecord(ev_views[k], s)))) return st;
+    if ((st = cuda_status(cudaEventRecord(ev_views[k], sp)))) return st;
     if ((st = cuda_status(cudaStreamWaitEvent(sb, ev_views[k], 0)))) return st;
     if ((st = parts ? bp(b, bp_lo, g.n_angle, kBpLast, sb) : bp(b, 0, 1 << 30, kBpWhole, sb)))
       return st;
@@ -747,7 +757,7 @@ LCT_API int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int
     for (int i = 1; i < 4; ++i)
       if ((st = cuda_status(cudaEventRecord(r->ev[i], s)))) return st;
     if ((st = streams_create(r->ss))) return st;
-    while (r->sev.size() < 5) {
+    while (r->sev.size() < (size_t)kForkJoinEvents) {
       cudaEvent_t e;
       if ((st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming)))) return st;
       r->sev.push_back(e);

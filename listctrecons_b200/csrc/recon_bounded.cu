@@ -454,11 +454,11 @@ struct ImageSink {
   SlabWriter* writer = nullptr;  // a file
 };
 
-// Events of one run: 5 for the fork and join, per slab: views ready, backprojected, downloaded;
+// Events of one run: kForkJoinEvents for the fork and join, per slab: views ready, backprojected, downloaded;
 // per piece: uploaded, packed.
 static int run_events(lct_recon* r, long long n_pieces, cudaEvent_t** base) {
   const int nb = r->info.n_blocks_run;
-  const size_t n_ev = 5 + 3 * (size_t)nb + 2 * (size_t)n_pieces;
+  const size_t n_ev = kForkJoinEvents + 3 * (size_t)nb + 2 * (size_t)n_pieces;
   while (r->sev.size() < n_ev) {
     cudaEvent_t e;
     int st = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -469,8 +469,10 @@ static int run_events(lct_recon* r, long long n_pieces, cudaEvent_t** base) {
   return LCT_OK;
 }
 
-static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink, cudaStream_t s,
-                        const StreamSet& ss) {
+static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink,
+                        cudaStream_t caller, const StreamSet& ss) {
+  (void)caller;                    // the caller forks the set from it and joins it back
+  const cudaStream_t s = ss.prep;  // per-piece rebin / filter / pack (high priority)
   const lct_geom& g = r->info.ctg;
   const lct_img& ig = r->info.ig;
   const int nb = r->info.n_blocks_run;
@@ -478,10 +480,11 @@ static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink
   const long long plane = r->plane;
   const long long P = r->piece > 0 ? r->piece : kDefaultPiece;
   int st;
-  const long long n_pieces = r->g_count / P + nb + 2;  // + the first slab's short piece
+  // + the first slab's short pieces (the pivot and at most 64 doublings up to a full piece)
+  const long long n_pieces = r->g_count / P + nb + 2 + 64;
   cudaEvent_t* ev = nullptr;
   if ((st = run_events(r, n_pieces, &ev))) return st;
-  cudaEvent_t* ev_views = ev + 5;
+  cudaEvent_t* ev_views = ev + kForkJoinEvents;
   cudaEvent_t* ev_bp = ev_views + nb;
   cudaEvent_t* ev_dl = ev_bp + nb;
   cudaEvent_t* ev_up = ev_dl + nb;
@@ -647,7 +650,7 @@ static int run_forked(lct_recon* r, cudaStream_t s, F body) {
   st = body();
   int st2 = streams_join(r->ss, s, r->sev.data() + 1);
   if (st) {
-    cudaStream_t all[5] = {r->ss.up, r->ss.down, r->ss.bp[0], r->ss.bp[1], s};
+    cudaStream_t all[7] = {r->ss.up, r->ss.down, r->ss.bp[0], r->ss.bp[1], r->ss.cnn, r->ss.prep, s};
     for (cudaStream_t x : all) cudaStreamSynchronize(x);
     return st;
   }

@@ -1,30 +1,41 @@
 // lct_recon internals shared by recon.cu and batch.cu (not part of the ABI).
 #pragma once
 
+#include <algorithm>
 #include <vector>
 
 #include "lct_internal.h"
 
 namespace lct {
 // The copy and compute streams of a streamed run: owned by a recon, or shared by a batch.
+// prep carries the per-piece rebin / filter / pack at the device's highest stream priority: the
+// block scheduler then hands it SMs as backprojection CTAs retire, so the views of later slabs
+// are ready before the running slab ends and consecutive slab launches overlap their tails
+// (at equal priority those kernels waited for the running grid's last wave).
 struct StreamSet {
-  cudaStream_t up = nullptr, down = nullptr, bp[2] = {}, cnn = nullptr;
+  cudaStream_t up = nullptr, down = nullptr, bp[2] = {}, cnn = nullptr, prep = nullptr;
 };
 int streams_create(StreamSet& ss);  // creates the missing streams (non-blocking)
 void streams_destroy(StreamSet& ss);
 // fork: every stream of the set waits for the work queued on s so far (ev records it);
-// join: s waits for every stream of the set (ev4: four events, recorded on the set's streams)
+// join: s waits for every stream of the set (ev5: five events, recorded on the set's streams)
+constexpr int kForkJoinEvents = 6;  // events a run keeps for its fork (1) and join (5)
 int streams_fork(const StreamSet& ss, cudaStream_t s, cudaEvent_t ev);
-int streams_join(const StreamSet& ss, cudaStream_t s, const cudaEvent_t* ev4);
+int streams_join(const StreamSet& ss, cudaStream_t s, const cudaEvent_t* ev5);
 
 // The first slab of a streamed run is backprojected in parts as its views arrive; a part needs
 // the conjugates (half a turn on) of its pairs.  The piece that crosses half a turn ends
-// kFirstPairs pairs past it, so the first part starts then and not up to a piece later.
+// kFirstPairs pairs past it, so the first part starts then and not up to a piece later, and the
+// pieces after it grow with the pairs already available (at least 2 kFirstPairs views) up to the
+// full piece: each part's views are uploaded and packed while the part before it runs, instead
+// of the backprojector waiting for a whole piece after a short first part.
 constexpr long long kFirstPairs = 64;
 inline long long first_part_target(long long done, long long target, long long gfirst,
                                    long long half) {
   const long long pivot = gfirst + half + kFirstPairs;
-  return done < pivot && target > pivot ? pivot : target;
+  if (done < pivot) return target > pivot ? pivot : target;
+  const long long grow = std::max<long long>(2 * kFirstPairs, done - (gfirst + half));
+  return std::min(target, done + grow);
 }
 
 // Pinned host staging: a 2 MiB-aligned anonymous mapping with transparent huge pages requested,

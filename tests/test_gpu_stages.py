@@ -119,7 +119,8 @@ def test_rebin_pi_ori_tex8_is_the_texture_unit_at_the_reference_coordinates(setu
     texture) sampled at the coordinates the oracle computes with the reference's FP32
     expressions.  The two coordinate computations differ only by FMA contraction and libm ulps,
     which can move an 8-bit weight by one step for a few samples; the software emulation above
-    is held only to 2e-3 because the unit's z combination is not reproduced exactly."""
+    is held only to 2e-3 because the unit's z combination is not reproduced exactly.  Measured
+    on B200: every sample identical (rel-L2 0)."""
     torch, g, fan = setup["torch"], setup["g"], setup["fan"]
     lib = capi.lib()
     d_fan = _dev(torch, fan)
@@ -137,7 +138,7 @@ def test_rebin_pi_ori_tex8_is_the_texture_unit_at_the_reference_coordinates(setu
     err = orc.rel_l2(got, hw)
     print(f"PI-original TEX8 vs texture unit at the reference's coordinates: rel_l2={err:.3e}, "
           f"identical samples {np.mean(got == hw):.5f}")
-    assert err < 1e-5
+    assert err < 1e-6
 
 
 def test_weight_pi_ori(setup):
