@@ -296,7 +296,7 @@ int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, lct_recon
    views are uploaded in pieces on an internal copy stream while earlier pieces are rebinned,
    filtered and backprojected slab by slab, and each finished slab is downloaded on a second copy
    stream (pinned host buffers make the copies asynchronous; a pageable volume is downloaded
-   once after the pipeline, or, for a bounded recon, copied out of pinned slabs by two threads,
+   once after the pipeline, or, for a bounded recon, copied out of pinned slabs by four threads,
    so the pipeline is never held by a copy into pageable memory).  The volume is bit-identical
    to the device-resident run. */
 int lct_recon_run(lct_recon* r, const float* fan, int64_t fan_view0, int fan_on_device,
@@ -320,12 +320,12 @@ int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
    and RawImageWriter (Src/ImageWriter.cpp:9-43) for every block of the run, with 64-bit offsets.
    fan_path: the DataInterpFile, fan view v of the scan at byte (v + DataOffset) * nt * ns * 4;
    four reader threads read the run's views into pinned chunks (whole views, at most 16 MiB)
-   that are uploaded as the pipeline needs them.  image_path (or NULL): the volume [n_blocks_run * 32][ny][nx] float32 is written
-   there slab by slab; image (or NULL): host buffer for the volume, pinned or pageable.  At least
-   one of the two.  A file, or a pageable buffer, is written from pinned slabs by two writer
-   threads (both outputs from one download per slab); a pinned buffer alone is downloaded into
-   directly.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
-   correction.  The recon's pinned staging (eight fan chunks, three slabs) is pinned slot by slot
+   that are uploaded as the pipeline needs them.  image_path (or NULL): the volume
+   [n_blocks_run * 32][ny][nx] float32 is written there slab by slab; image (or NULL): host
+   buffer for the volume, pinned or pageable.  At least one of the two.  A file, or a pageable
+   buffer, is written from pinned slabs by four writer threads (both outputs from one download
+   per slab); a pinned buffer alone is downloaded into directly.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
+   correction.  The recon's pinned staging (eight fan chunks, four slabs) is pinned slot by slot
    by the reader and writer threads on first use, overlapped with the run, and kept until
    lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
 int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,

@@ -98,8 +98,10 @@ constexpr int kFanStage = 8;              // pinned fan chunks of lct_recon_run_
 constexpr long long kFanChunkBytes = 16LL << 20;  // a chunk: whole views, at most 16 MiB (>= 1 view)
 constexpr int kFanReaders = 4;            // reader threads (chunk c on thread c mod 4)
 static_assert(kFanStage % kFanReaders == 0, "slot s must belong to reader s mod kFanReaders");
-constexpr int kImgStage = 3;              // pinned slabs of the slab writer
-constexpr int kSinkThreads = 2;           // slab writer threads (file writes, pageable copies)
+constexpr int kImgStage = 4;              // pinned slabs of the slab writer
+constexpr int kSinkThreads = 4;           // slab writer threads (file writes, pageable copies:
+                                          // first-touch page faults of a fresh host volume
+                                          // spread over the threads)
 
 // Fan views a global parallel view g reads lie in [g + lo, g + hi] (scan rebin shifts, FP64).
 static void rebin_reach(const lct_geom& g, long long& lo, long long& hi) {
@@ -272,7 +274,7 @@ class FanReader {
 
 // ----------------------------------------------------------------------------------------------
 // writer: device slab -> pinned slot (D2H on the download stream) -> file and/or pageable host
-// volume (two threads)
+// volume (four threads)
 // ----------------------------------------------------------------------------------------------
 class SlabWriter {
  public:
