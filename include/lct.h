@@ -324,10 +324,11 @@ int lct_recon_device_bytes(const lct_recon* r, int64_t* bytes);
    [n_blocks_run * 32][ny][nx] float32 is written there slab by slab; image (or NULL): host
    buffer for the volume, pinned or pageable.  At least one of the two.  A file, or a pageable
    buffer, is written from pinned slabs by four writer threads (both outputs from one download
-   per slab); a pinned buffer alone is downloaded into directly.  Scan-mode recons as for lct_recon_create_bounded (bounded or not), no learned
-   correction.  The recon's pinned staging (eight fan chunks, four slabs) is pinned slot by slot
-   by the reader and writer threads on first use, overlapped with the run, and kept until
-   lct_recon_destroy.  Synchronous; LCT_ERR_IO for a missing or short file. */
+   per slab); a pinned buffer alone is downloaded into directly.  Scan-mode recons as for
+   lct_recon_create_bounded (bounded or not), no learned correction.  The recon's pinned staging
+   (eight fan chunks, four slabs) is pinned slot by slot by the reader and writer threads on
+   first use, overlapped with the run, and kept until lct_recon_destroy.  Synchronous;
+   LCT_ERR_IO for a missing or short file. */
 int lct_recon_run_file(lct_recon* r, const char* fan_path, const char* image_path, float* image,
                        lct_stream stream);
 /* File I/O of the last lct_recon_run_file, seconds: s3[0] = time the reader threads spent in
