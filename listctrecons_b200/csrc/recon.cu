@@ -541,9 +541,7 @@ int streams_create(StreamSet& ss) {
     if (st) return st;
   }
   if (!ss.prep) {
-    int least = 0, greatest = 0;
-    int st = cuda_status(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    if (!st) st = cuda_status(cudaStreamCreateWithPriority(&ss.prep, cudaStreamNonBlocking, greatest));
+    const int st = cuda_status(cudaStreamCreateWithFlags(&ss.prep, cudaStreamNonBlocking));
     if (st) return st;
   }
   return LCT_OK;
@@ -590,7 +588,7 @@ int recon_run_streamed(lct_recon* r, const float* fan_host, long long skip, floa
   const long long slab = (long long)kBlockSlices * ig.nx * ig.ny;
   const long long plane = r->plane;
   int st;
-  const cudaStream_t sp = ss.prep;  // per-piece rebin / filter / pack (high priority)
+  const cudaStream_t sp = ss.prep;  // per-piece rebin / filter / pack
   (void)s;                          // the caller forks the set from s and joins it back
   // events: the caller's fork and join, per slab: views ready, backprojected, corrected;
   // per piece: uploaded, packed

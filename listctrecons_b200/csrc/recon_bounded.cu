@@ -474,7 +474,7 @@ static int run_events(lct_recon* r, long long n_pieces, cudaEvent_t** base) {
 static int run_pipeline(lct_recon* r, const FanFeed& feed, const ImageSink& sink,
                         cudaStream_t caller, const StreamSet& ss) {
   (void)caller;                    // the caller forks the set from it and joins it back
-  const cudaStream_t s = ss.prep;  // per-piece rebin / filter / pack (high priority)
+  const cudaStream_t s = ss.prep;  // per-piece rebin / filter / pack
   const lct_geom& g = r->info.ctg;
   const lct_img& ig = r->info.ig;
   const int nb = r->info.n_blocks_run;

@@ -8,10 +8,10 @@
 
 namespace lct {
 // The copy and compute streams of a streamed run: owned by a recon, or shared by a batch.
-// prep carries the per-piece rebin / filter / pack at the device's highest stream priority: the
-// block scheduler then hands it SMs as backprojection CTAs retire, so the views of later slabs
-// are ready before the running slab ends and consecutive slab launches overlap their tails
-// (at equal priority those kernels waited for the running grid's last wave).
+// prep carries the per-piece rebin / filter / pack of streamed runs, apart from the caller's
+// stream (measured on config 2 host to host: 85.5 -> 84.3 ms per volume with the first slab's
+// growing pieces; the device's highest stream priority for it measured 0.4-0.7% slower on the
+// same box, on config 2 and on the bounded config 5).
 struct StreamSet {
   cudaStream_t up = nullptr, down = nullptr, bp[2] = {}, cnn = nullptr, prep = nullptr;
 };
