@@ -16,8 +16,10 @@
 // EXACT also: floor, fraction and index of a sample from one round-down add (no conversions)
 // and one wide multiply-add for its address; per-view terms staged in shared memory 128 views
 // at a time; a warp-uniform path without out tests, selects or row clamps when a chunk's first
-// and last slices project inside the detector rows; an L1 prefetch of the next view's tile
-// footprint; a polynomial asin on tiles within dso / 2 of the axis.
+// and last slices project inside the detector rows, where the view and its conjugate run as
+// packed FP32 pairs (FFMA2 / FADD2: half the instructions for the row, floor, fraction and first
+// two bilinear FMAs of the two samples, each lane rounded as in the scalar form); an L1 prefetch
+// of the next view's tile footprint; a polynomial asin on tiles within dso / 2 of the axis.
 #include <climits>
 #include <cmath>
 #include <mutex>
@@ -86,8 +88,9 @@ __global__ void __launch_bounds__(256) quad_pack_kernel(const float* __restrict_
     const int i = q - 2;
     const float t00 = texel(j, i), t01 = texel(j, i + 1), t10 = texel(j + 1, i),
                 t11 = texel(j + 1, i + 1);
-    // differences: a bilinear sample is then T00 + a dx + b (dy + a dxy), three FMAs
-    out[q] = make_float4(t00, t01 - t00, t10 - t00, (t11 - t10) - (t01 - t00));
+    // differences {T00, dy, dx, dxy}: a bilinear sample is then T00 + a dx + b (dy + a dxy), the
+    // pair (T00, dy) + a (dx, dxy) one packed FMA
+    out[q] = make_float4(t00, t10 - t00, t01 - t00, (t11 - t10) - (t01 - t00));
   }
 }
 
@@ -125,15 +128,15 @@ __device__ __forceinline__ float quad_sample(const float4* __restrict__ qb, int 
   float b = yb - fy;
   int j = (int)fy;
   j = min(max(j, -2), nt);
-  const float4 v = __ldg(qb + (j + 2) * qcols);  // T00, dx, dy, dxy
+  const float4 v = __ldg(qb + (j + 2) * qcols);  // T00, dy, dx, dxy
   if (INTERP == LCT_INTERP_TEX8) {
     // texture unit: w01 = a - w11, w10 = b - w11, w00 = 1 - a - b + w11, so the sample is
     // T00 + a dx + b dy + w11 dxy with w11 = round-half-up(a b) on the 1/256 grid
     b = q8(b);
     const float w11 = floorf(a * b * 256.0f + 0.5f) * (1.0f / 256.0f);
-    return fmaf(w11, v.w, fmaf(b, v.z, fmaf(a, v.y, v.x)));
+    return fmaf(w11, v.w, fmaf(b, v.y, fmaf(a, v.z, v.x)));
   }
-  return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
+  return fmaf(b, fmaf(a, v.w, v.y), fmaf(a, v.z, v.x));
 }
 
 // EXACT floor without conversions: for |x| < 2^22, x + 1.5 * 2^23 rounded toward -inf is
@@ -162,8 +165,16 @@ __device__ __forceinline__ float quad_sample_exact(unsigned long long col, unsig
   int rb = __float_as_int(t);
   if (CLAMP) rb = min(max(rb, kMagicBits), kMagicBits + nt + 2);
   const float4 v = __ldg(reinterpret_cast<const float4*>(
-      col + (unsigned long long)(unsigned)rb * qrow_bytes));  // T00, dx, dy, dxy
-  return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
+      col + (unsigned long long)(unsigned)rb * qrow_bytes));  // T00, dy, dx, dxy
+  return fmaf(b, fmaf(a, v.w, v.y), fmaf(a, v.z, v.x));
+}
+
+// Blackwell's packed FP32 pairs (FFMA2, FADD2, FMUL2): one instruction for two lanes, each lane
+// rounded exactly as the scalar operation; x - y is written fma(y, -1, x), one rounding like the
+// subtraction.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 f2sub(float2 x, float2 y) {
+  return __ffma2_rn(y, make_float2(-1.0f, -1.0f), x);
 }
 
 // EXACT column: weight a and 16 * (clamped column bit pattern) added to the biased view base
@@ -429,8 +440,27 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
                    fabsf(h2) <= wt && fabsf(e2) <= wt;
         }
         if (__all_sync(0xffffffffu, inside)) {
+          // the two views of the pair as one packed FP32 pair per slice: each lane is
+          // slice_x(j, inside) rounded the same way
+          const float2 KD = make_float2(kd1, kd2), H = make_float2(h1, h2), U = make_float2(u1, u2);
+          const float2 A1 = f2(a1), A2 = f2(a2);
 #pragma unroll
-          for (int j = 0; j < NZ; ++j) slice_x(j, std::true_type{});
+          for (int j = 0; j < NZ; ++j) {
+            const float2 J = f2((float)j);
+            const float2 qh = __ffma2_rn(J, KD, H);
+            const float w1 = -qh.y * __fdividef(1.0f, qh.x - qh.y);
+            const float2 u = __ffma2_rn(J, KD, U);
+            const float2 t = __fadd2_rd(u, f2(kMagic));
+            const float2 b = f2sub(u, __fadd2_rn(t, f2(-kMagic)));
+            const float4 v0 = __ldg(reinterpret_cast<const float4*>(
+                q1 + (unsigned long long)(unsigned)__float_as_int(t.x) * A.qrow_bytes));
+            const float4 v1 = __ldg(reinterpret_cast<const float4*>(
+                q2 + (unsigned long long)(unsigned)__float_as_int(t.y) * A.qrow_bytes));
+            const float2 p0 = __ffma2_rn(A1, make_float2(v0.z, v0.w), make_float2(v0.x, v0.y));
+            const float2 p1 = __ffma2_rn(A2, make_float2(v1.z, v1.w), make_float2(v1.x, v1.y));
+            const float s1 = fmaf(b.x, p0.y, p0.x), s2 = fmaf(b.y, p1.y, p1.x);
+            acc[j] = fmaf(w1, s1 - s2, acc[j] + s2);
+          }
         } else {
 #pragma unroll
           for (int j = 0; j < NZ; ++j)
@@ -683,7 +713,7 @@ __device__ __forceinline__ void bp_tma_tile(const BpQuadArgs& A, const CUtensorM
         const float4 v = smem ? lds128(sq0 + (uint32_t)rb * kTmaRowBytes)
                               : __ldg(reinterpret_cast<const float4*>(
                                     gq + (unsigned long long)(unsigned)rb * A.qrow_bytes));
-        return fmaf(b, fmaf(a, v.w, v.z), fmaf(a, v.y, v.x));
+        return fmaf(b, fmaf(a, v.w, v.y), fmaf(a, v.z, v.x));  // T00, dy, dx, dxy
       };
       auto slice_x = [&](int j, auto inside, auto smem) {
         const float fj = (float)j;

@@ -80,10 +80,11 @@ int launch_bp_par(const lct_geom& g, const lct_img& ig, const BpLaunch& L, cudaS
 
 // Filtered views in quad layout for the backprojector.  Per view, entry (j, i) for
 // j in [-2, nt], i in [-2, ns] (stored at (j + 2) * (ns + 3) + (i + 2)) holds the 2 x 2 texel
-// block with top-left (j, i) as {T00, T01 - T00, T10 - T00, T11 - T10 - T01 + T00}, texels
-// outside the detector read as 0 (LCT_ADDR_BORDER) or clamped to the edge (LCT_ADDR_CLAMP).
-// A bilinear sample is then one 16-byte load at its clamped origin and three FMAs; the padding
-// ring makes every clamped origin valid.
+// block with top-left (j, i) as {T00, T10 - T00, T01 - T00, T11 - T10 - T01 + T00} (row
+// difference before column difference), texels outside the detector read as 0 (LCT_ADDR_BORDER)
+// or clamped to the edge (LCT_ADDR_CLAMP).  A bilinear sample is then one 16-byte load at its
+// clamped origin and three FMAs -- the first two, (T00, dy) + a (dx, dxy), as one packed FP32
+// pair; the padding ring makes every clamped origin valid.
 LCT_HD inline long long quad_cols(int ns) { return (long long)ns + 3; }
 LCT_HD inline long long quad_view_elems(int ns, int nt) { return (long long)(nt + 3) * (ns + 3); }
 // ring > 0: quads is a ring of `ring` views and rows view v is packed into slot
