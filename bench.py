@@ -346,6 +346,70 @@ def oracle_accuracy(w, plan, fan, f0, img, interp, slabs, ystep=1):
 PLAIN_RUNS = 3  # runs of each program in the plain_gpu leg (median reported)
 
 
+def rel_l2(a, b) -> float:
+    """||a - b|| / ||b|| in FP64."""
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    n = float(np.dot(b, b))
+    d = float(np.dot(a - b, a - b))
+    return (d / n) ** 0.5 if n > 0 else d ** 0.5
+
+
+def pi_window_in_bounds(plan) -> bool:
+    """The reference's PI-window backprojector walks forward to a_min + n_proj_turn / 2 with no
+    bound against n_angle (CUDA/Backprojector.cu:225), reading betas[ia] past the end of its
+    array when a window reaches beyond the block's views.  a_min <= a_middle, so the largest index
+    is at most a_middle + n_proj_turn / 2: the reference program runs its PI configuration only
+    when that stays below n_angle for every slice."""
+    g, ig = plan.info.ctg, plan.info.ig
+    dzv = np.float32(g.pitch) / np.float32(g.n_proj_turn)
+    for iz in range(ig.nz):
+        zc = np.float32((iz - ig.wz) * ig.dz)
+        a_mid = min(max(int(np.round((zc - np.float32(g.source_z0)) / dzv)), 0), g.n_angle - 1)
+        if a_mid + g.n_proj_turn // 2 > g.n_angle - 1:
+            return False
+    return True
+
+
+def pi_original_library(geo, blocks, fan_d, upd_pi):
+    """The library's PI-original chain (lct_recon in block mode: PI-original rebin, its
+    pre-weighting, the filter, the PI-window backprojector) on the workload's blocks from a
+    device-resident fan, CUDA-event timed: in the reference's sampling (TEX8, FP32 filter) and in
+    the exact mode (exact interpolation, BF16x6 filter).  Each entry keeps its volume under
+    "image" for the comparison with the reference program."""
+    import torch
+
+    from listctrecons_b200 import capi
+    from listctrecons_b200.recon import Plan, Reconstruction
+
+    params = geo.scan_params()
+    params.first_block, params.max_blocks = 0, blocks  # the workload's blocks of the scan
+    plan = Plan(params=params, angles32=geo.angles32(), zpos32=geo.zpos32())
+    out = {}
+    for name, kw in (("tex8_fp32", dict(interp=capi.INTERP_TEX8, filter_mode=capi.FILTER_FP32)),
+                     ("exact_bf16x6", dict(interp=capi.INTERP_EXACT,
+                                           filter_mode=capi.FILTER_BF16X6))):
+        rec = Reconstruction(plan, mode=capi.MODE_BLOCK, rebinner=capi.REBIN_PI_ORI,
+                             preweight=capi.PW_PI_ORI, backprojector=capi.BP_PI_ORI, **kw)
+        img = torch.empty(rec.image_shape, dtype=torch.float32, device="cuda")
+        rec.run(fan_d, img)  # warm-up
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(reps):
+            rec.run(fan_d, img)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"value": upd_pi / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_volume": ms,
+                     "image": img.cpu().numpy().ravel()}
+        del rec, img
+        torch.cuda.empty_cache()
+    return out
+
+
 def plain_gpu(w, geo, ph, ours_value):
     """The reference program built from its own sources (oracle/_ref/ref_timed) on the same scan,
     and the typed drop-in program (reference host code + the product) with both factory type
@@ -368,9 +432,17 @@ def plain_gpu(w, geo, ph, ours_value):
     plan = Plan(g2)
     nb_all = plan.info.n_blocks
     upd = Reconstruction(plan).stats().voxel_updates * w["blocks"] / nb_all
-    fan = simulate_gpu(g2, ph, i0=1e5, seed=7).cpu().numpy()
+    ig = plan.info.ig
+    # PI-window backprojection: n_proj_turn / 2 + 1 view samples per voxel (the two loops of
+    # CUDA/Backprojector.cu:197-246 visit a_middle .. a_min + na1_half)
+    upd_pi = float(w["blocks"]) * 32 * ig.ny * ig.nx * (plan.info.ctg.n_proj_turn // 2 + 1)
+    fan_d = simulate_gpu(g2, ph, i0=1e5, seed=7)
+    pi_lib = pi_original_library(g2, w["blocks"], fan_d, upd_pi)
+    fan = fan_d.cpu().numpy()
+    del fan_d
     torch.cuda.empty_cache()
     runs = {}
+    images = {}
     with tempfile.TemporaryDirectory() as td:
         prm = write_scan_files(g2, fan, Path(td) / "data", Path(td) / "out")
         del fan
@@ -378,15 +450,25 @@ def plain_gpu(w, geo, ph, ours_value):
         if typed.exists():
             cmds += [("dropin_stages", [str(typed), str(prm), "Helicalfdkramprebingpu"]),
                      ("dropin_b200", [str(typed), str(prm), "Helicalfdkramprebinb200"])]
+        pi_ok = pi_window_in_bounds(plan)
+        if pi_ok:  # the reference's alternate (PI-original) configuration, both programs
+            cmds += [("reference_pi", [str(ref), str(prm), "pi"])]
+            if typed.exists():
+                cmds += [("dropin_pi", [str(typed), str(prm), "Helicalfdkpiorigpu"])]
         # each program PLAIN_RUNS times, interleaved; the median run is reported (host-side
         # costs -- file reads, pinning, freeing -- scatter from run to run on a shared host)
         samples = {name: [] for name, _ in cmds}
-        for _ in range(PLAIN_RUNS):
+        nslices = w["blocks"] * 32
+        for it in range(PLAIN_RUNS):
             for name, cmd in cmds:
                 r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
                 if r.returncode != 0:
                     runs[name] = {"unavailable": f"{name} failed: " + r.stdout[-300:]}
                     continue
+                if it == 0 and name in ("reference", "dropin_stages", "reference_pi", "dropin_pi"):
+                    # the workload's slabs of each program's volume, for the parity records
+                    images[name] = np.fromfile(Path(td) / "out" / "image.raw", dtype=np.float32,
+                                               count=nslices * ig.ny * ig.nx)
                 rec = json.loads(r.stdout.strip().splitlines()[-1])
                 m = re.search(r"\[B200\] create ([0-9.]+) s, run ([0-9.]+) s, destroy ([0-9.]+) s; "
                               r"reads ([0-9.]+) s .*waits for reads ([0-9.]+) s, for the writer "
@@ -402,12 +484,50 @@ def plain_gpu(w, geo, ph, ours_value):
             smp.sort(key=lambda x: x[0])
             sec, nblk, split = smp[len(smp) // 2]
             secs = sec * w["blocks"] / nblk
-            runs[name] = {"value": upd / secs / 1e9, "unit": UNIT, "s_per_volume": secs,
+            u = upd_pi if name.endswith("_pi") else upd
+            runs[name] = {"value": u / secs / 1e9, "unit": UNIT, "s_per_volume": secs,
                           "blocks_timed": nblk, "runs": len(smp),
                           "reconstruct_seconds_all": [round(x[0], 4) for x in smp]}
             if split:
                 runs[name]["split_s"] = split
+    pi = {"library": pi_lib}
+    if not pi_ok:
+        pi["reference"] = {"unavailable": "a PI window would pass the end of the reference's betas "
+                           "(no bound against n_angle, CUDA/Backprojector.cu:225)"}
+    for name in ("reference_pi", "dropin_pi"):
+        if name in runs:
+            pi[name.replace("_pi", "")] = runs.pop(name)
+    if "value" in pi.get("reference", {}):
+        for k in ("dropin", "library"):
+            for v in ([pi.get(k)] if k == "dropin" else list(pi["library"].values())):
+                if isinstance(v, dict) and "value" in v:
+                    v["speedup_vs_reference"] = v["value"] / pi["reference"]["value"]
+    if "reference_pi" in images:
+        ref_img = images["reference_pi"]
+        if "dropin_pi" in images:
+            pi["dropin_vs_reference"] = {"rel_l2": rel_l2(images["dropin_pi"], ref_img),
+                                         "max_abs": float(np.abs(images["dropin_pi"] - ref_img).max())}
+        for k, v in pi["library"].items():
+            if isinstance(v, dict) and "image" in v:
+                img = v.pop("image")
+                v["vs_reference_program"] = {"rel_l2": rel_l2(img, ref_img),
+                                             "max_abs": float(np.abs(img - ref_img).max())}
+    for v in pi["library"].values():
+        if isinstance(v, dict):
+            v.pop("image", None)
+    pi["what"] = ("the reference's alternate configuration (Src/ReconstructorAbstractFactory.cpp:"
+                  "19-22: PI-original rebin, cone-angle pre-weighting, ramp filter, PI-window "
+                  "backprojection) on the same scan: the reference program (its own kernels), the "
+                  "typed drop-in (Helicalfdkpiorigpu, the reference's per-block flow), and the "
+                  "library's block-mode chain device-resident; voxel-GUPS here counts the PI "
+                  "window's n_proj_turn / 2 + 1 samples per voxel")
+    if "reference" in images and "dropin_stages" in images and "value" in runs.get("dropin_stages", {}):
+        a, b = images["dropin_stages"], images["reference"]
+        runs["dropin_stages"]["vs_reference_program"] = {"rel_l2": rel_l2(a, b),
+                                                         "max_abs": float(np.abs(a - b).max()),
+                                                         "slices": nslices}
     out = runs.pop("reference")
+    out["pi_original"] = pi
     if "value" in out:
         out["speedup_e2e"] = ours_value / out["value"]
         out["what"] = ("reference program (all Src/*.cpp + CUDA/*.cu built from its sources, "

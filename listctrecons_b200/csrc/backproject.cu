@@ -44,7 +44,8 @@ struct BpArgsDev {
   int slab_view[kBpMaxSlabs];
   int slab_z0[kBpMaxSlabs];
   int a_min[kBpMaxZ], a_mid[kBpMaxZ], a_max[kBpMaxZ];
-  float pitch;  // PI-window kernel only
+  float pitch;     // PI-window kernel only
+  int trig_table;  // PI-window kernel: 1 = every view's cos / sin staged in dynamic shared memory
 };
 
 struct ColSetup {
@@ -113,6 +114,22 @@ __device__ __forceinline__ void view_trig(const float* __restrict__ betas, int v
   s = (float)sd;
 }
 
+// The view trigonometry of a sampling mode: TEX8 (the reference's sampling) takes the
+// reference's own __cosf / __sinf of the FP32 angle (CUDA/Backprojector.cu:53, 61-62, 203-204,
+// 228-229), whose error grows with the angle (absolute errors near 1e-5 at the 63 rad of ten
+// rotations); EXACT takes view_trig.
+template <int INTERP>
+__device__ __forceinline__ void view_trig_mode(const float* __restrict__ betas, int v, float& c,
+                                               float& s) {
+  if (INTERP == LCT_INTERP_TEX8) {
+    const float b = __ldg(betas + v);
+    c = __cosf(b);
+    s = __sinf(b);
+  } else {
+    view_trig(betas, v, c, s);
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Pairs kernel (full windows).
 // grid (ceil(nx/32), ceil(ny/8), n_slabs * zchunks), block (32, 8)
@@ -152,8 +169,8 @@ __global__ void __launch_bounds__(kBpTX* kBpTY) bp_par_pairs_kernel(const __grid
     __syncthreads();
     if (tid < kBpVB && vb + tid < vhi) {
       const int ia = vb + tid;
-      view_trig(betas, ia, s_c1[tid], s_s1[tid]);
-      view_trig(betas, ia + A.half, s_c2[tid], s_s2[tid]);
+      view_trig_mode<INTERP>(betas, ia, s_c1[tid], s_s1[tid]);
+      view_trig_mode<INTERP>(betas, ia + A.half, s_c2[tid], s_s2[tid]);
       int jlo = nzc, jhi = 0;
       for (int j = 0; j < nzc; ++j)
         if (ia >= A.a_min[z0 + j] && ia < A.a_mid[z0 + j]) {
@@ -265,11 +282,11 @@ __global__ void __launch_bounds__(kBpTX* kBpTY) bp_par_general_kernel(const __gr
     __syncthreads();
     if (tid < kBpVB && vb + tid < vhi) {
       const int ia = vb + tid;
-      view_trig(betas, ia, s_c[0][tid], s_s[0][tid]);
+      view_trig_mode<INTERP>(betas, ia, s_c[0][tid], s_s[0][tid]);
       // a conjugate past the last view samples outside the array (border: 0); its angle is
       // taken from the last view so no read leaves the caller's betas[n_angle]
-      view_trig(betas, min(ia + A.half, last), s_c[1][tid], s_s[1][tid]);
-      view_trig(betas, max(ia - A.half, 0), s_c[2][tid], s_s[2][tid]);
+      view_trig_mode<INTERP>(betas, min(ia + A.half, last), s_c[1][tid], s_s[1][tid]);
+      view_trig_mode<INTERP>(betas, max(ia - A.half, 0), s_c[2][tid], s_s[2][tid]);
       int jlo = nzc, jhi = 0;
       for (int j = 0; j < nzc; ++j)
         if (ia >= A.a_min[z0 + j] && ia < A.a_max[z0 + j]) {
@@ -355,11 +372,21 @@ __global__ void __launch_bounds__(kBpTX* kBpTY) bp_par_general_kernel(const __gr
 // sums its views in the reference's order (backward from a_middle, then forward from
 // a_middle + 1), with the reference's expression for t (CUDA/Backprojector.cu:200-245).
 constexpr int kPiNZ = 8;
+constexpr int kPiTrigMaxViews = 12288;  // 96 KB of staged view trigonometry per CTA
 template <int INTERP, int ADDR>
 __global__ void __launch_bounds__(256) bp_pi_ori_z_kernel(const __grid_constant__ BpArgsDev A) {
+  extern __shared__ float2 s_trig[];  // trig_table: cos, sin of view v at s_trig[v]
   const int ix = blockIdx.x * kBpTX + threadIdx.x;
   const int iy = blockIdx.y * kBpTY + threadIdx.y;
   const int z0 = blockIdx.z * kPiNZ;
+  if (A.trig_table) {  // once per CTA instead of once per thread and view; the same values
+    for (int v = threadIdx.y * kBpTX + threadIdx.x; v < A.n_angle; v += kBpTX * kBpTY) {
+      float c, sn;
+      view_trig_mode<INTERP>(A.betas, v, c, sn);
+      s_trig[v] = make_float2(c, sn);
+    }
+    __syncthreads();
+  }
   if (ix >= A.nx || iy >= A.ny) return;
   const int nzc = min(kPiNZ, A.nz - z0);
   const float xc = ((float)ix - A.wx) * A.dx;
@@ -393,7 +420,13 @@ __global__ void __launch_bounds__(256) bp_pi_ori_z_kernel(const __grid_constant_
   auto terms = [&](int v) {
     ViewTerms w;
     float cb, sb;
-    view_trig(A.betas, v, cb, sb);
+    if (A.trig_table) {
+      const float2 t = s_trig[v];
+      cb = t.x;
+      sb = t.y;
+    } else {
+      view_trig_mode<INTERP>(A.betas, v, cb, sb);
+    }
     const float s = -xc * cb - yc * sb;
     const float gamma = asinf(s / A.dso);
     w.temp1 = sqrtf(A.dso * A.dso - s * s);
@@ -453,6 +486,7 @@ __global__ void __launch_bounds__(256) bp_pi_ori_z_kernel(const __grid_constant_
 // host side
 // ---------------------------------------------------------------------------------------
 static void fill_common(BpArgsDev& d, const lct_geom& g, const lct_img& ig) {
+  d.trig_table = 0;
   d.ns = g.ns;
   d.nt = g.nt;
   d.n_angle = g.n_angle;
@@ -637,13 +671,22 @@ LCT_API int lct_backproject_pi_ori(const lct_geom* g, const lct_img* ig, const f
   dim3 block(kBpTX, kBpTY);
   cudaStream_t s = (cudaStream_t)stream;
   bool tex = interp == LCT_INTERP_TEX8, clamp = addr == LCT_ADDR_CLAMP;
-  if (tex && clamp)
-    bp_pi_ori_z_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP><<<grid, block, 0, s>>>(a);
-  else if (tex)
-    bp_pi_ori_z_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER><<<grid, block, 0, s>>>(a);
-  else if (clamp)
-    bp_pi_ori_z_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP><<<grid, block, 0, s>>>(a);
-  else
-    bp_pi_ori_z_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER><<<grid, block, 0, s>>>(a);
-  return launch_status();
+  // the view trig table in shared memory (8 bytes per view) up to kPiTrigMaxViews views; longer
+  // blocks evaluate it per thread and view, with the same values
+  const size_t smem = (size_t)g->n_angle * sizeof(float2);
+  a.trig_table = g->n_angle <= kPiTrigMaxViews ? 1 : 0;
+  const size_t dyn = a.trig_table ? smem : 0;
+  auto launch = [&](auto kernel) {
+    if (dyn > 48 * 1024) {
+      int e = cuda_status(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)dyn));
+      if (e) return e;
+    }
+    kernel<<<grid, block, dyn, s>>>(a);
+    return launch_status();
+  };
+  if (tex && clamp) return launch(bp_pi_ori_z_kernel<LCT_INTERP_TEX8, LCT_ADDR_CLAMP>);
+  if (tex) return launch(bp_pi_ori_z_kernel<LCT_INTERP_TEX8, LCT_ADDR_BORDER>);
+  if (clamp) return launch(bp_pi_ori_z_kernel<LCT_INTERP_EXACT, LCT_ADDR_CLAMP>);
+  return launch(bp_pi_ori_z_kernel<LCT_INTERP_EXACT, LCT_ADDR_BORDER>);
 }

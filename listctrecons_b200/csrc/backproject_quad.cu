@@ -42,6 +42,20 @@ __device__ __forceinline__ void view_trig_pi(const float* __restrict__ betas, in
   s = (float)sd;
 }
 
+// TEX8 (the reference's sampling) takes the reference's own __cosf / __sinf of the FP32 view
+// angle (CUDA/Backprojector.cu:53, 61-62); EXACT the FP64 view_trig_pi
+template <int INTERP>
+__device__ __forceinline__ void view_trig_mode(const float* __restrict__ betas, int v, float& c,
+                                               float& s) {
+  if (INTERP == LCT_INTERP_TEX8) {
+    const float b = __ldg(betas + v);
+    c = __cosf(b);
+    s = __sinf(b);
+  } else {
+    view_trig_pi(betas, v, c, s);
+  }
+}
+
 struct BpQuadArgs {
   const float4* quads;  // slab s's local view ia is view slab_view[s] + ia of quads (mod qring)
   long long qring;      // > 0: quads is a ring of qring views; 0: linear
@@ -324,8 +338,8 @@ __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by
     if (tid < kQVB && vb + tid < vhi) {
       const int ia = vb + tid;
       float c1, s1, c2, s2;
-      view_trig_pi(betas, ia, c1, s1);
-      view_trig_pi(betas, ia + A.half, c2, s2);
+      view_trig_mode<INTERP>(betas, ia, c1, s1);
+      view_trig_mode<INTERP>(betas, ia + A.half, c2, s2);
       s_cs[tid] = make_float4(c1, s1, c2, s2);
       const float4* v1 = RING ? quad_view_ptr(A, sv, ia) : quads + (long long)ia * A.qstride;
       const float4* v2 = RING ? quad_view_ptr(A, sv, ia + A.half)
@@ -863,8 +877,8 @@ __device__ __forceinline__ void bp_tex_tile(const BpQuadArgs& A, cudaTextureObje
     if (tid < kQVB && vb + tid < vhi) {
       const int ia = vb + tid;
       float c1, s1, c2, s2;
-      view_trig_pi(betas, ia, c1, s1);
-      view_trig_pi(betas, ia + A.half, c2, s2);
+      view_trig_mode<LCT_INTERP_TEX8>(betas, ia, c1, s1);
+      view_trig_mode<LCT_INTERP_TEX8>(betas, ia + A.half, c2, s2);
       s_cs[tid] = make_float4(c1, s1, c2, s2);
       long long v1 = (long long)sv + ia, v2 = v1 + A.half;
       if (A.qring > 0) {

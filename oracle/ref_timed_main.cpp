@@ -8,6 +8,11 @@
  * times reconstruct() (wall clock around a device synchronisation) so the plain FP32 GPU
  * path can be reported beside the product.  Its stdout banners are the reference's own;
  * the last line is a JSON record.
+ *
+ * `ref_timed <prm> pi` builds the reference's alternate configuration instead, the one its
+ * factory has commented out (Src/ReconstructorAbstractFactory.cpp:19-22): the FDKReconstructor
+ * over PiOriRebiner, PiOriPreWeighting, RampFilterGPU and PiOriBackprojectorGPU, all the
+ * reference's own classes and kernels.
  */
 #include <cuda_runtime.h>
 
@@ -15,21 +20,29 @@
 #include <cstdio>
 #include <string>
 
+#include "Backprojector.h"
 #include "DataStructs.h"
 #include "FileParams.h"
+#include "Filter.h"
 #include "ImageWriter.h"
+#include "PreWeighting.h"
+#include "Rebiner.h"
 #include "Reconstructor.h"
 #include "ReconstructorAbstractFactory.h"
 
 int main(int argc, char** argv) {
   if (argc < 2) {
-    std::fprintf(stderr, "usage: ref_timed <prm>\n");
+    std::fprintf(stderr, "usage: ref_timed <prm> [pi]\n");
     return 1;
   }
   FileParams* fp = new FileParams(std::string(argv[1]));
   ReconData* mr = new ReconData(*fp);
   ReconstrctorAbstractFactory* fac = new ReconstrctorAbstractFactory();
-  Reconstructor* recon = fac->createReconstructor("Helicalfdkramprebingpu");
+  const bool pi = argc >= 3 && std::string(argv[2]) == "pi";
+  Reconstructor* recon =
+      pi ? new FDKReconstructor(new PiOriRebiner(), new RampFilterGPU(), new PiOriBackprojectorGPU(),
+                                new PiOriPreWeighting())
+         : fac->createReconstructor("Helicalfdkramprebingpu");
   cudaDeviceSynchronize();
   auto t0 = std::chrono::steady_clock::now();
   recon->reconstruct(mr);
@@ -38,8 +51,8 @@ int main(int argc, char** argv) {
   ImageWriter* w = new RawImageWriter();
   w->writeImage(mr);
   double s = std::chrono::duration<double>(t1 - t0).count();
-  std::printf("{\"reconstruct_seconds\": %.6f, \"n_blocks\": %d, \"cuda_error\": %d}\n", s,
-              mr->ri_()->n_blocks(), (int)err);
+  std::printf("{\"reconstruct_seconds\": %.6f, \"n_blocks\": %d, \"cuda_error\": %d, \"chain\": \"%s\"}\n",
+              s, mr->ri_()->n_blocks(), (int)err, pi ? "pi_original" : "fan2par");
   delete w;
   delete recon;
   delete fac;

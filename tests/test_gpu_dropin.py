@@ -121,3 +121,44 @@ def test_factory_types_through_the_reference_interfaces(cuda, tmp_path):
     print(f"whole-scan type (exact, bf16x6, bounded) vs FP64 oracle: rel_l2={err:.3e}; "
           f"vs reference program {orc.rel_l2(fast, ref):.3e}")
     assert fast.size == oracle.size and err < 1e-4
+
+
+@pytest.mark.skipif(not (TYPED.exists() and REF.exists()), reason="builds need the reference tree")
+def test_pi_original_type_matches_the_references_pi_configuration(cuda, tmp_path):
+    """The reference's alternate configuration (Src/ReconstructorAbstractFactory.cpp:19-22:
+    PiOriRebiner, PiOriPreWeighting, RampFilterGPU, PiOriBackprojectorGPU), built from the
+    reference's own classes and kernels (`ref_timed <prm> pi`), against the same configuration on
+    the drop-in stages (`LISTCTRecons_b200 <prm> Helicalfdkpiorigpu`: the PI-original rebin sampled
+    by the texture unit, the FP32 filter in the reference's order, the PI-window backprojector),
+    same scan and files.  The reference's PI window has no bound against n_angle
+    (CUDA/Backprojector.cu:225); on this scan a_middle + n_proj_turn / 2 stays below n_angle for
+    every slice, so its view index never passes the end of its betas."""
+    from listctrecons_b200.recon import Plan
+    from listctrecons_b200.scan import write_scan_files
+    from tests.golden.make_gpu_golden import small_scan
+
+    geo, _, fan = small_scan()
+    p = Plan(geo)
+    g, ig = p.info.ctg, p.info.ig
+    dzv = np.float32(g.pitch) / np.float32(g.n_proj_turn)
+    for iz in range(ig.nz):  # the bound above, checked on the host before the reference runs
+        zc = np.float32((iz - ig.wz) * ig.dz)
+        a_mid = min(max(int(np.round((zc - np.float32(g.source_z0)) / dzv)), 0), g.n_angle - 1)
+        assert a_mid + g.n_proj_turn // 2 <= g.n_angle - 1
+    prm = write_scan_files(geo, fan, tmp_path / "data", tmp_path / "ref")
+    r = subprocess.run([str(REF), str(prm), "pi"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-1500:]
+    assert json_last(r.stdout)["chain"] == "pi_original"
+    ref = np.fromfile(tmp_path / "ref" / "image.raw", dtype=np.float32)
+    img, rec = _typed_run(prm, tmp_path / "pi", "Helicalfdkpiorigpu", {"LCT_DROPIN_FILTER": "fp32"})
+    assert rec["type"] == "Helicalfdkpiorigpu"
+    err = orc.rel_l2(img, ref)
+    print(f"PI-original type vs the reference's PI configuration: rel_l2={err:.3e}, "
+          f"max_abs={np.abs(img - ref).max():.3e}")
+    assert img.size == ref.size and np.isfinite(ref).all() and err < 1e-4
+
+
+def json_last(stdout: str) -> dict:
+    import json
+
+    return json.loads(stdout.strip().splitlines()[-1])
