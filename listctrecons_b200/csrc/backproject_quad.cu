@@ -31,7 +31,9 @@
 
 namespace lct {
 
-constexpr int kQTX = 32, kQTY = 8, kQVB = 128;  // views staged per batch
+// tile 16 x 16 voxel columns (warps of 16 x 2): its footprint on the detector, |16 cos| + |16 sin|
+// voxels wide, averages 20% narrower over the views than a 32 x 8 tile's; kQVB views staged per batch
+constexpr int kQTX = 16, kQTY = 16, kQVB = 128;
 
 // cos/sin of a view angle in FP64 rounded to float (sincospi: no large-argument reduction)
 __device__ __forceinline__ void view_trig_pi(const float* __restrict__ betas, int v, float& c,
@@ -270,7 +272,7 @@ __device__ __forceinline__ void quad_col(float p_idx, int ns, int& off, float& a
   off = min(max(i, -2), ns) + 2;
 }
 
-// One tile: voxel columns [bx*32, +32) x [by*8, +8), slab/slice chunk bz.  Called with
+// One tile: voxel columns [bx*kQTX, +kQTX) x [by*kQTY, +kQTY), slab/slice chunk bz.  Called with
 // CTA-uniform arguments by every thread of a 256-thread CTA.
 template <int NZ, int INTERP, bool PART, bool RING>
 __device__ __forceinline__ void bp_quad_tile(const BpQuadArgs& A, int bx, int by, int bz) {
