@@ -106,15 +106,25 @@ int launch_bp_par_texture(const lct_geom& g, const lct_img& ig, const BpLaunch& 
                           cudaTextureObject_t tex, cudaStream_t s);
 // A 3-D float texture of `depth` filtered views (x = column, y = row, z = view slot) with linear
 // filtering and BORDER or CLAMP addressing; filled from linear views by view_texture_fill
-// (slot0 onward, wrapping at depth).
+// (slot0 onward, wrapping at depth).  view_texture_add_other_mode adds a second texture object
+// over the same array with the other addressing; view_texture_for picks the one for `addr`
+// (0 when that mode has none).
 struct ViewTexture {
   cudaArray_t arr = nullptr;
   cudaTextureObject_t tex = 0;
+  cudaTextureObject_t tex_other = 0;
+  int addr = 0;
   int ns = 0, nt = 0;
   long long depth = 0;
 };
 int view_texture_create(ViewTexture& t, int ns, int nt, long long depth, int addr);
+int view_texture_add_other_mode(ViewTexture& t);
+cudaTextureObject_t view_texture_for(const ViewTexture& t, int addr);
 void view_texture_destroy(ViewTexture& t);
+// PI-original rebin sampled by the texture unit from a caller-owned texture of the fan block
+// (depth >= n_angle_add): fills it and launches on s, stream-ordered, no allocation
+int launch_rebin_pi_ori_tex(const lct_geom& g, const ViewTexture& t, int addr, const float* d_fan,
+                            float* d_par, cudaStream_t s);
 int view_texture_fill(const ViewTexture& t, const float* rows, long long views, long long slot0,
                       cudaStream_t s);
 // True when every slice window of the block is a full rotation (the pairs kernels apply).

@@ -483,6 +483,16 @@ __global__ void __launch_bounds__(256) rebin_pi_ori_tex_kernel(cudaTextureObject
   }
 }
 
+int lct::launch_rebin_pi_ori_tex(const lct_geom& g, const ViewTexture& t, int addr,
+                                 const float* d_fan, float* d_par, cudaStream_t s) {
+  const cudaTextureObject_t tex = view_texture_for(t, addr);
+  if (!tex || t.ns != g.ns || t.nt != g.nt || t.depth < g.n_angle_add) return LCT_ERR_ARG;
+  int st = view_texture_fill(t, d_fan, g.n_angle_add, 0, s);
+  if (st) return st;
+  rebin_pi_ori_tex_kernel<<<dim3(g.n_angle, g.nt), 256, 0, s>>>(tex, d_par, rebin_args(g));
+  return launch_status();
+}
+
 LCT_API int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par, int interp,
                              int addr, lct_stream stream) {
   int st = check_geom(g);
@@ -498,11 +508,7 @@ LCT_API int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par
     // CUDA/Rebiner.cu:181-230); released after the kernel, so this mode synchronises the stream
     ViewTexture t;
     if ((st = view_texture_create(t, g->ns, g->nt, g->n_angle_add, addr))) return st;
-    st = view_texture_fill(t, d_fan, g->n_angle_add, 0, s);
-    if (!st) {
-      rebin_pi_ori_tex_kernel<<<grid, 256, 0, s>>>(t.tex, d_par, a);
-      st = launch_status();
-    }
+    st = launch_rebin_pi_ori_tex(*g, t, addr, d_fan, d_par, s);
     const int st2 = cuda_status(cudaStreamSynchronize(s));
     view_texture_destroy(t);
     return st ? st : st2;

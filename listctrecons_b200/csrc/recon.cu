@@ -39,6 +39,7 @@ static void free_recon(lct_recon* r) {
   cudaFree(r->d_img);
   cudaFree(r->d_quad);
   view_texture_destroy(r->vtex);
+  view_texture_destroy(r->pi_tex);
   cudaFree(r->d_tc);
   cudaFree(r->d_plain);
   for (auto& e : r->ev)
@@ -212,6 +213,18 @@ LCT_API int lct_recon_create(const lct_plan* plan, const lct_recon_opts* opts, l
     if (r->quads && !r->tex_bp &&
         (st = alloc((void**)&r->d_quad, sizeof(float4) * par_views * quad_view_elems(g.ns, g.nt))))
       break;
+    if (o.rebinner == LCT_REBIN_PI_ORI && o.interp == LCT_INTERP_TEX8) {
+      // the fan block as a 3-D texture once per recon, with both addressings (legacy addressing
+      // clamps the first block), instead of an array allocated and freed per block
+      if ((st = view_texture_create(r->pi_tex, g.ns, g.nt, g.n_angle_add, LCT_ADDR_BORDER)) ||
+          (st = view_texture_add_other_mode(r->pi_tex))) {
+        if (st != LCT_ERR_UNSUPPORTED) break;
+        view_texture_destroy(r->pi_tex);  // beyond the texture limits: the per-call path
+        st = LCT_OK;
+      } else {
+        r->device_bytes += (long long)sizeof(float) * g.n_angle_add * r->plane;
+      }
+    }
     if (r->tma_bp && bp_tma_map(&r->tma_map, r->d_quad, g.ns, g.nt, par_views) != LCT_OK)
       r->tma_bp = false;  // no tensor-map encoder in this driver: the L1 quad kernel
     if (o.filter_mode != LCT_FILTER_FP32) r->tc_rows = par_views * g.nt;
@@ -336,7 +349,10 @@ static int run_rebin(lct_recon* r, const lct_geom& g, const float* fan_block, fl
   const int interp = r->o.interp;
   switch (r->o.rebinner) {
     case LCT_REBIN_NULL: return lct_rebin_null(&g, fan_block, par, addr, s);
-    case LCT_REBIN_PI_ORI: return lct_rebin_pi_ori(&g, fan_block, par, interp, addr, s);
+    case LCT_REBIN_PI_ORI:
+      if (interp == LCT_INTERP_TEX8 && r->pi_tex.arr)  // the recon's own texture of the fan block
+        return launch_rebin_pi_ori_tex(g, r->pi_tex, addr, fan_block, par, s);
+      return lct_rebin_pi_ori(&g, fan_block, par, interp, addr, s);
     default: return lct_rebin_fan2par(&g, fan_block, par, interp, addr, s);
   }
 }

@@ -69,6 +69,7 @@ struct lct_recon {
   bool quads = false;        // full windows: the pairs kernels (quads or texture) apply
   bool tex_bp = false;       // the pairs backprojection samples a 3-D texture (TEX8) instead
   lct::ViewTexture vtex;     // filtered views as that texture (scan: global views; block: one block)
+  lct::ViewTexture pi_tex;   // PI-original rebin in TEX8: the fan block as a texture, reused per block
   bool tma_bp = false;       // EXACT pairs backprojection with TMA-staged footprints (same quads)
   CUtensorMap tma_map;       // d_quad as the staged kernel's tensor
   cudaEvent_t ev[6] = {};

@@ -6,6 +6,19 @@
 
 namespace lct {
 
+static int make_tex_object(cudaArray_t arr, int addr, cudaTextureObject_t* out) {
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = arr;
+  cudaTextureDesc td = {};
+  const cudaTextureAddressMode m = addr == LCT_ADDR_CLAMP ? cudaAddressModeClamp : cudaAddressModeBorder;
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = m;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 0;
+  return cuda_status(cudaCreateTextureObject(out, &rd, &td, nullptr));
+}
+
 int view_texture_create(ViewTexture& t, int ns, int nt, long long depth, int addr) {
   if (ns <= 0 || nt <= 0 || depth <= 0) return LCT_ERR_ARG;
   int dev = 0, maxw = 0, maxh = 0, maxd = 0;
@@ -17,16 +30,8 @@ int view_texture_create(ViewTexture& t, int ns, int nt, long long depth, int add
   cudaChannelFormatDesc desc = cudaCreateChannelDesc<float>();
   int st = cuda_status(cudaMalloc3DArray(&t.arr, &desc, make_cudaExtent(ns, nt, (size_t)depth)));
   if (st) return st;
-  cudaResourceDesc rd = {};
-  rd.resType = cudaResourceTypeArray;
-  rd.res.array.array = t.arr;
-  cudaTextureDesc td = {};
-  const cudaTextureAddressMode m = addr == LCT_ADDR_CLAMP ? cudaAddressModeClamp : cudaAddressModeBorder;
-  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = m;
-  td.filterMode = cudaFilterModeLinear;
-  td.readMode = cudaReadModeElementType;
-  td.normalizedCoords = 0;
-  if ((st = cuda_status(cudaCreateTextureObject(&t.tex, &rd, &td, nullptr)))) {
+  t.addr = addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  if ((st = make_tex_object(t.arr, t.addr, &t.tex))) {
     cudaFreeArray(t.arr);
     t.arr = nullptr;
     return st;
@@ -37,8 +42,21 @@ int view_texture_create(ViewTexture& t, int ns, int nt, long long depth, int add
   return LCT_OK;
 }
 
+int view_texture_add_other_mode(ViewTexture& t) {
+  if (!t.arr) return LCT_ERR_ARG;
+  if (t.tex_other) return LCT_OK;
+  return make_tex_object(t.arr, t.addr == LCT_ADDR_CLAMP ? LCT_ADDR_BORDER : LCT_ADDR_CLAMP,
+                         &t.tex_other);
+}
+
+cudaTextureObject_t view_texture_for(const ViewTexture& t, int addr) {
+  const int a = addr == LCT_ADDR_CLAMP ? LCT_ADDR_CLAMP : LCT_ADDR_BORDER;
+  return a == t.addr ? t.tex : t.tex_other;
+}
+
 void view_texture_destroy(ViewTexture& t) {
   if (t.tex) cudaDestroyTextureObject(t.tex);
+  if (t.tex_other) cudaDestroyTextureObject(t.tex_other);
   if (t.arr) cudaFreeArray(t.arr);
   t = ViewTexture();
 }

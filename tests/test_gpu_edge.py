@@ -95,3 +95,47 @@ def test_pi_original_chain_matches_fp64_oracle(ragged):
     err = orc.rel_l2(img, ref)
     print(f"PI-original chain: rel_l2 {err:.2e}")
     assert err < 1e-4
+
+
+@pytest.mark.parametrize("addr", [capi.ADDR_BORDER, capi.ADDR_LEGACY])
+def test_pi_original_tex8_recon_matches_the_stage_chain(ragged, addr):
+    """Block-mode PI-original chain in TEX8: lct_recon keeps one texture of the fan block for all
+    its blocks (both addressings on one array; legacy addressing clamps the first block), the
+    stage entry point lct_rebin_pi_ori binds a texture per call as the reference does.  Same
+    kernels, same texels: the volumes are bit-identical."""
+    import ctypes as C
+
+    import torch
+
+    p, fan = ragged
+    g, ig = p.info.ctg, p.info.ig
+    lib = capi.load()
+    rec = Reconstruction(p, mode=capi.MODE_BLOCK, interp=capi.INTERP_TEX8, addr=addr,
+                         rebinner=capi.REBIN_PI_ORI, preweight=capi.PW_PI_ORI,
+                         backprojector=capi.BP_PI_ORI, filter_mode=capi.FILTER_FP32)
+    img = rec.run(fan).cpu().numpy()
+    taps = np.zeros(2 * g.ns, dtype=np.float32)  # the recon's own taps (lct_recon_opts defaults)
+    capi.check(lib.lct_filter_taps(capi.FILTER_RAMLAK, capi.WINDOW_NONE, g.ns, g.ds,
+                                   taps.ctypes.data))
+    h = torch.from_numpy(taps).cuda()
+    slab = 32 * ig.ny * ig.nx
+    ref = np.empty(p.info.n_blocks_run * slab, dtype=np.float32)
+    par = torch.empty(g.n_angle * g.nt * g.ns, dtype=torch.float32, device="cuda")
+    out = torch.empty(slab, dtype=torch.float32, device="cuda")
+    for b, bi in enumerate(p.blocks[: p.info.n_blocks_run]):
+        a = capi.ADDR_CLAMP if (addr == capi.ADDR_LEGACY and b == 0) else capi.ADDR_BORDER
+        blk = fan[bi.block_proj_start: bi.block_proj_start + g.n_angle_add].contiguous()
+        betas = torch.from_numpy(np.ascontiguousarray(
+            p.angles32[bi.block_proj_start + g.add_projections:][: g.n_angle])).cuda()
+        capi.check(lib.lct_rebin_pi_ori(C.byref(g), blk.data_ptr(), par.data_ptr(),
+                                        capi.INTERP_TEX8, a, None))
+        capi.check(lib.lct_weight_pi_ori(C.byref(g), par.data_ptr(), None))
+        capi.check(lib.lct_filter_rows(g.ns, h.data_ptr(), par.data_ptr(), g.n_angle * g.nt,
+                                       capi.FILTER_FP32, None))
+        capi.check(lib.lct_backproject_pi_ori(C.byref(g), C.byref(ig), betas.data_ptr(),
+                                              par.data_ptr(), out.data_ptr(), capi.INTERP_TEX8,
+                                              a, None))
+        torch.cuda.synchronize()
+        ref[b * slab:(b + 1) * slab] = out.cpu().numpy()
+    assert np.isfinite(img).all()
+    np.testing.assert_array_equal(img.ravel(), ref)
