@@ -107,7 +107,8 @@ int lct_rebin_null(const lct_geom* g, const float* d_fan, float* d_par, int addr
                    lct_stream stream);
 /* PiOriRebiner::rebin + rebin_pi_ori_kernel (CUDA/Rebiner.cu:156-233).  TEX8 samples the fan
    block through the texture unit as the reference does (its trilinear filter, a 3-D array bound
-   for the call) and therefore synchronises the stream before returning; EXACT is asynchronous. */
+   for the call) and therefore synchronises the stream before returning; EXACT is asynchronous.
+   (lct_recon in block mode keeps one such array for all its blocks and stays asynchronous.) */
 int lct_rebin_pi_ori(const lct_geom* g, const float* d_fan, float* d_par, int interp, int addr,
                      lct_stream stream);
 
@@ -149,7 +150,8 @@ int lct_filter_rows(int ns, const float* d_h, float* d_rows, int64_t nrows, int 
  * (device, radians, float as in the reference), img [nz][ny][nx] (device).
  * ------------------------------------------------------------------------------------- */
 /* HelicalConeBeamFanRebinBackprojectorGPU::backproject + backprojection_cbct_par_kernel
-   (CUDA/Backprojector.cu:12-169; na1_half = n_proj_turn/2, dz per view = pitch/n_proj_turn). */
+   (CUDA/Backprojector.cu:12-169; na1_half = n_proj_turn/2, dz per view = pitch/n_proj_turn).
+   TEX8 takes the reference's own __cosf / __sinf of the view angle, EXACT FP64 trigonometry. */
 int lct_backproject_par(const lct_geom* g, const lct_img* ig, const float* d_betas,
                         const float* d_proj, float* d_img, int interp, int addr,
                         lct_stream stream);
@@ -171,7 +173,8 @@ int lct_backproject_par_noalloc(const lct_geom* g, const lct_img* ig, const floa
                                 const float* d_proj, float* d_img, int interp, int addr,
                                 lct_stream stream);
 /* PiOriBackprojectorGPU::backproject + backprojection_cbct_pi_ori_kernel
-   (CUDA/Backprojector.cu:171-307). */
+   (CUDA/Backprojector.cu:171-307).  TEX8 takes the reference's own __cosf / __sinf of the view
+   angle, EXACT FP64 trigonometry; the walk stops at the last of the n_angle views. */
 int lct_backproject_pi_ori(const lct_geom* g, const lct_img* ig, const float* d_betas,
                            const float* d_proj, float* d_img, int interp, int addr,
                            lct_stream stream);
